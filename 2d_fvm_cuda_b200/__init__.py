@@ -1,0 +1,15 @@
+"""B200-native split 2D Euler finite-volume solver (sm_100a kernels behind a C ABI).
+
+The package directory name starts with a digit, so import it with
+``importlib.import_module("2d_fvm_cuda_b200")``.
+
+* ``RGRP_2D_CUDA``, ``ghostCellStrategy``, ``precision`` -- the reference's
+  solver interface (src/wrappers.cuh:17-65) over libfvm2d.so.
+* ``Handle`` -- one C-ABI solver handle (include/fvm2d.h), for callers that
+  want the state to stay on the GPU between calls.
+* ``scenarios`` -- initial data (the reference's demo problems and seeded
+  workloads).
+"""
+from . import scenarios  # noqa: F401
+from ._lib import FP64, FP64_STRICT, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
+from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

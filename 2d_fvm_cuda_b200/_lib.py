@@ -1,0 +1,161 @@
+"""ctypes binding of lib/libfvm2d.so (the C ABI declared in include/fvm2d.h).
+
+The library is built in-tree (`make -C 2d_fvm_cuda_b200`).  There is no
+fallback: if the shared object is missing or a call fails, an exception
+says why.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libfvm2d.so")
+
+FVM2D_OK, FVM2D_ERR_INVALID, FVM2D_ERR_CUDA, FVM2D_ERR_STATE = 0, 1, 2, 3
+FP64, FP64_STRICT = 0, 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+# (name, restype, argtypes) of every entry point in include/fvm2d.h
+SIGNATURES = [
+    ("fvm2d_last_error", ctypes.c_char_p, []),
+    ("fvm2d_version", ctypes.c_char_p, []),
+    ("fvm2d_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int]),
+    ("fvm2d_destroy", ctypes.c_int, [_vp]),
+    ("fvm2d_set_spatial_layout", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    ("fvm2d_set_time_layout", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    ("fvm2d_set_end_time", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_set_cfl", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_set_alpha", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_set_gamma", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_set_ghost_strategy", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("fvm2d_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("fvm2d_set_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("fvm2d_set_rp_initial_data", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    ("fvm2d_get_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("fvm2d_solve", ctypes.c_int, [_vp]),
+    ("fvm2d_advance", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_get_computation_time_ms", ctypes.c_int, [_vp, _dp]),
+    ("fvm2d_get_time_stages_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
+]
+
+_LIB = None
+
+
+class FVM2DError(RuntimeError):
+    """A libfvm2d call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libfvm2d error {code}: {msg}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """Loads libfvm2d.so once; raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}` "
+                "(the CUDA library is required; there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def check(rc: int) -> None:
+    if rc != FVM2D_OK:
+        raise FVM2DError(rc, load().fvm2d_last_error().decode())
+
+
+def as_cells(U) -> np.ndarray:
+    """(ny, nx, 4|5) float64 C-contiguous view/copy of a state."""
+    A = np.ascontiguousarray(U, dtype=np.float64)
+    if A.ndim != 3 or A.shape[2] not in (4, 5):
+        raise ValueError("a state is an array of shape (ny, nx, 4) or (ny, nx, 5)")
+    return A
+
+
+class Handle:
+    """Owns one fvm2d_solver.  Thin: every method is one C call."""
+
+    def __init__(self, nx: int, ny: int):
+        self.lib = load()
+        self.nx, self.ny = int(nx), int(ny)
+        h = _vp()
+        check(self.lib.fvm2d_create(ctypes.byref(h), self.nx, self.ny))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.fvm2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, width=1.0, height=1.0, t_end=0.0, cfl=0.5, alpha=1.9, gamma=1.4,
+                  strategy=0, precision=FP64) -> None:
+        check(self.lib.fvm2d_set_spatial_layout(self.h, width, height))
+        check(self.lib.fvm2d_set_time_layout(self.h, t_end, cfl))
+        check(self.lib.fvm2d_set_alpha(self.h, alpha))
+        check(self.lib.fvm2d_set_gamma(self.h, gamma))
+        check(self.lib.fvm2d_set_ghost_strategy(self.h, int(strategy)))
+        check(self.lib.fvm2d_set_precision(self.h, int(precision)))
+
+    def set_state(self, U) -> None:
+        A = as_cells(U)
+        if A.shape[:2] != (self.ny, self.nx):
+            raise ValueError(f"state shape {A.shape[:2]} does not match ({self.ny}, {self.nx})")
+        check(self.lib.fvm2d_set_state(self.h, A.ctypes.data, A.shape[2]))
+
+    def set_state_ptr(self, ptr: int, stride: int) -> None:
+        """Uploads from a raw host or device pointer of ny*nx*stride doubles."""
+        check(self.lib.fvm2d_set_state(self.h, ptr, stride))
+
+    def get_state(self, stride: int = 4, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.ny, self.nx, stride))
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (self.ny, self.nx, stride)
+        check(self.lib.fvm2d_get_state(self.h, out.ctypes.data, stride))
+        return out
+
+    def get_state_ptr(self, ptr: int, stride: int) -> None:
+        check(self.lib.fvm2d_get_state(self.h, ptr, stride))
+
+    def solve(self) -> None:
+        check(self.lib.fvm2d_solve(self.h))
+
+    def advance(self, n: int) -> int:
+        k = ctypes.c_int(0)
+        check(self.lib.fvm2d_advance(self.h, int(n), ctypes.byref(k)))
+        return k.value
+
+    def time(self):
+        t = ctypes.c_double(0)
+        s = ctypes.c_int(0)
+        dt = ctypes.c_double(0)
+        check(self.lib.fvm2d_get_time(self.h, ctypes.byref(t), ctypes.byref(s), ctypes.byref(dt)))
+        return t.value, s.value, dt.value
+
+    def computation_time_ms(self) -> float:
+        ms = ctypes.c_double(0)
+        check(self.lib.fvm2d_get_computation_time_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def time_stages_count(self) -> int:
+        c = ctypes.c_longlong(0)
+        check(self.lib.fvm2d_get_time_stages_count(self.h, ctypes.byref(c)))
+        return c.value

@@ -1,0 +1,433 @@
+// fvm2d_capi.cu -- host runtime behind include/fvm2d.h.
+//
+// A handle owns, on one device:
+//   U        the state: 4 planes (rho, p, u, v), rows padded to `pitch`
+//            elements (a multiple of 32) so every row starts 256-byte aligned;
+//   scratch  two more state-sized buffers (A, B) that the sweeps write, also
+//            used as the staging area for uploads and downloads;
+//   ctl      the device-resident StepControl of the time loop;
+//   a CUDA graph of GRAPH_STEPS steps (5 kernels each) replayed until the
+//   control record says the loop has ended, so the only host round trip is
+//   one 64-byte read per graph replay (the reference reads the max wave
+//   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
+#include "../../include/fvm2d.h"
+#include "fvm2d_control.h"
+
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using fvm2d::LaunchConfig;
+using fvm2d::StepControl;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(FVM2D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);                   \
+    } while (0)
+
+struct Variant {
+    cudaError_t (*prepare)();
+    cudaError_t (*init)(const LaunchConfig &, cudaStream_t);
+    cudaError_t (*plan)(const LaunchConfig &, cudaStream_t);
+    cudaError_t (*step)(const LaunchConfig &, cudaStream_t);
+};
+
+const Variant kVariants[] = {
+    {fvm2d::fp64::prepare, fvm2d::fp64::enqueue_init, fvm2d::fp64::enqueue_plan, fvm2d::fp64::enqueue_step},
+    {fvm2d::fp64_strict::prepare, fvm2d::fp64_strict::enqueue_init, fvm2d::fp64_strict::enqueue_plan,
+     fvm2d::fp64_strict::enqueue_step},
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// AoS (stride doubles per cell, row-major) <-> SoA planes with a row pitch.
+__global__ void aos_to_soa(const double *__restrict__ in, int stride, double *__restrict__ U, int nx, int ny,
+                           int pitch, long long plane)
+{
+    const long long n = (long long)nx * ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int y = int(k / nx), x = int(k % nx);
+        const long long o = (long long)y * pitch + x;
+        for (int f = 0; f < 4; ++f) U[f * plane + o] = in[k * stride + f];
+    }
+}
+
+__global__ void soa_to_aos(const double *__restrict__ U, int nx, int ny, int pitch, long long plane, int stride,
+                           double *__restrict__ out)
+{
+    const long long n = (long long)nx * ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int y = int(k / nx), x = int(k % nx);
+        const long long o = (long long)y * pitch + x;
+        for (int f = 0; f < 4; ++f) out[k * stride + f] = U[f * plane + o];
+        for (int f = 4; f < stride; ++f) out[k * stride + f] = 0.0;
+    }
+}
+
+bool is_device_pointer(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+} // namespace
+
+struct fvm2d_solver {
+    int device = 0;
+    int nx = 0, ny = 0, pitch = 0;
+    long long plane = 0;
+    double width = 1.0, height = 1.0, t_end = 0.0, cfl = 0.5, alpha = 1.9, gamma = 1.4;
+    int strategy = FVM2D_OUTFLOW;
+    int precision = FVM2D_FP64;
+    cudaStream_t stream = nullptr;
+    double *U = nullptr;
+    double *scratch = nullptr;  // A then B
+    StepControl *ctl = nullptr;
+    StepControl *ctl_h = nullptr;  // pinned mirror
+    cudaGraphExec_t graph = nullptr;
+    int graph_variant = -1;
+    int graph_steps = 16;
+    bool have_state = false;
+    bool need_init = true;
+    double last_ms = 0.0;
+    long long total_steps = 0;
+
+    LaunchConfig config() const
+    {
+        LaunchConfig c;
+        c.nx = nx;
+        c.ny = ny;
+        c.pitch = pitch;
+        c.plane = plane;
+        c.U = U;
+        c.A = scratch;
+        c.B = scratch + 4 * plane;
+        c.ctl = ctl;
+        c.hx = width / double(nx);
+        c.hy = height / double(ny);
+        c.rhx = 1.0 / c.hx;
+        c.rhy = 1.0 / c.hy;
+        c.alpha = alpha;
+        c.gamma = gamma;
+        c.strategy = strategy;
+        c.plan.t_end = t_end;
+        c.plan.cfl = cfl;
+        c.plan.hmin = (c.hy < c.hx) ? c.hy : c.hx;
+        return c;
+    }
+
+    void drop_graph()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_variant = -1;
+    }
+
+    int build_graph()
+    {
+        if (graph && graph_variant == precision) return FVM2D_OK;
+        drop_graph();
+        const LaunchConfig c = config();
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < graph_steps && e == cudaSuccess; ++k) e = kVariants[precision].step(c, stream);
+        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e, "capture of the step kernels");
+        }
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            graph = nullptr;
+            return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        graph_variant = precision;
+        return FVM2D_OK;
+    }
+
+    // Replays the step graph until the control record says no step is in
+    // flight.  The record on the device must already be planned.
+    int loop()
+    {
+        int rc = build_graph();
+        if (rc) return rc;
+        auto t0 = std::chrono::high_resolution_clock::now();
+        for (;;) {
+            CK(cudaGraphLaunch(graph, stream));
+            CK(cudaMemcpyAsync(ctl_h, ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            if (!ctl_h->active) break;
+        }
+        auto t1 = std::chrono::high_resolution_clock::now();
+        last_ms = std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count() / 1000.0;
+        return FVM2D_OK;
+    }
+
+    int upload_control()
+    {
+        CK(cudaMemcpyAsync(ctl, ctl_h, sizeof(StepControl), cudaMemcpyHostToDevice, stream));
+        return FVM2D_OK;
+    }
+};
+
+namespace {
+
+int check(fvm2d_solver *s)
+{
+    if (!s) return fail(FVM2D_ERR_INVALID, "null solver handle");
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    return FVM2D_OK;
+}
+
+int upload(fvm2d_solver *s, const double *cells, int stride)
+{
+    const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
+    const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
+    aos_to_soa<<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, s->U, s->nx, s->ny, s->pitch, s->plane);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    s->have_state = true;
+    s->need_init = true;
+    std::memset(s->ctl_h, 0, sizeof(StepControl));
+    return FVM2D_OK;
+}
+
+} // namespace
+
+extern "C" {
+#pragma GCC visibility push(default)
+
+const char *fvm2d_last_error(void) { return g_err.c_str(); }
+
+const char *fvm2d_version(void) { return "fvm2d-b200 0.1 (sm_100a)"; }
+
+int fvm2d_create(fvm2d_solver **out, int nx, int ny)
+{
+    if (!out) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (nx < 6 || ny < 6) return fail(FVM2D_ERR_INVALID, "nx and ny must be at least 6 (two ghost layers per side)");
+    if ((long long)nx * ny > (1ll << 31) - 1) return fail(FVM2D_ERR_INVALID, "nx * ny must stay below 2^31");
+    fvm2d_solver *s = new (std::nothrow) fvm2d_solver();
+    if (!s) return fail(FVM2D_ERR_INVALID, "out of host memory");
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(e, "cudaGetDevice");
+    }
+    s->nx = nx;
+    s->ny = ny;
+    s->pitch = (nx + 31) / 32 * 32;
+    s->plane = (long long)s->pitch * ny;
+    const size_t state_bytes = sizeof(double) * 4 * (size_t)s->plane;
+    int rc = FVM2D_OK;
+    do {
+        for (int v = 0; v < kNumVariants && !rc; ++v)
+            if ((e = kVariants[v].prepare()) != cudaSuccess) rc = cuda_fail(e, "kernel attributes");
+        if (rc) break;
+        if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) { rc = cuda_fail(e, "cudaStreamCreate"); break; }
+        if ((e = cudaMalloc(&s->U, state_bytes))) { rc = cuda_fail(e, "cudaMalloc(state)"); break; }
+        if ((e = cudaMalloc(&s->scratch, 2 * state_bytes))) { rc = cuda_fail(e, "cudaMalloc(scratch)"); break; }
+        if ((e = cudaMalloc(&s->ctl, sizeof(StepControl)))) { rc = cuda_fail(e, "cudaMalloc(control)"); break; }
+        if ((e = cudaMallocHost(&s->ctl_h, sizeof(StepControl)))) { rc = cuda_fail(e, "cudaMallocHost"); break; }
+        std::memset(s->ctl_h, 0, sizeof(StepControl));
+        if ((e = cudaMemsetAsync(s->U, 0, state_bytes, s->stream))) { rc = cuda_fail(e, "cudaMemset"); break; }
+        if ((e = cudaMemsetAsync(s->scratch, 0, 2 * state_bytes, s->stream))) { rc = cuda_fail(e, "cudaMemset"); break; }
+        if ((e = cudaMemsetAsync(s->ctl, 0, sizeof(StepControl), s->stream))) { rc = cuda_fail(e, "cudaMemset"); break; }
+        if ((e = cudaStreamSynchronize(s->stream))) { rc = cuda_fail(e, "cudaStreamSynchronize"); break; }
+    } while (0);
+    if (rc) {
+        fvm2d_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return FVM2D_OK;
+}
+
+int fvm2d_destroy(fvm2d_solver *s)
+{
+    if (!s) return FVM2D_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->drop_graph();
+    if (s->U) cudaFree(s->U);
+    if (s->scratch) cudaFree(s->scratch);
+    if (s->ctl) cudaFree(s->ctl);
+    if (s->ctl_h) cudaFreeHost(s->ctl_h);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FVM2D_OK;
+}
+
+#define SETTER(name, field, type, cond, msg)                                  \
+    int name(fvm2d_solver *s, type v)                                          \
+    {                                                                          \
+        if (int rc = check(s)) return rc;                                      \
+        if (!(cond)) return fail(FVM2D_ERR_INVALID, msg);                      \
+        s->field = v;                                                          \
+        s->drop_graph();                                                       \
+        return FVM2D_OK;                                                       \
+    }
+
+SETTER(fvm2d_set_end_time, t_end, double, v == v, "end time must be a number")
+SETTER(fvm2d_set_cfl, cfl, double, v > 0.0, "CFL must be positive")
+SETTER(fvm2d_set_alpha, alpha, double, v == v, "alpha must be a number")
+SETTER(fvm2d_set_gamma, gamma, double, v > 1.0, "gamma must exceed 1")
+SETTER(fvm2d_set_ghost_strategy, strategy, int, v >= FVM2D_OUTFLOW && v <= FVM2D_REFLECTIVE_TB,
+       "unknown ghost-cell strategy")
+SETTER(fvm2d_set_precision, precision, int, v >= 0 && v < kNumVariants, "unknown precision")
+
+int fvm2d_set_spatial_layout(fvm2d_solver *s, double width, double height)
+{
+    if (int rc = check(s)) return rc;
+    if (!(width > 0.0 && height > 0.0)) return fail(FVM2D_ERR_INVALID, "width and height must be positive");
+    s->width = width;
+    s->height = height;
+    s->drop_graph();
+    return FVM2D_OK;
+}
+
+int fvm2d_set_time_layout(fvm2d_solver *s, double end_time, double cfl)
+{
+    if (int rc = fvm2d_set_end_time(s, end_time)) return rc;
+    return fvm2d_set_cfl(s, cfl);
+}
+
+int fvm2d_set_state(fvm2d_solver *s, const double *cells, int stride)
+{
+    if (int rc = check(s)) return rc;
+    if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
+    if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
+    return upload(s, cells, stride);
+}
+
+int fvm2d_set_rp_initial_data(fvm2d_solver *s, const double *U1, const double *U2, const double *U3,
+                              const double *U4)
+{
+    if (int rc = check(s)) return rc;
+    if (!U1 || !U2 || !U3 || !U4) return fail(FVM2D_ERR_INVALID, "null quadrant state");
+    std::vector<double> cells;
+    try {
+        cells.resize((size_t)s->nx * s->ny * 4);
+    } catch (...) {
+        return fail(FVM2D_ERR_INVALID, "out of host memory");
+    }
+    for (int j = 0; j < s->ny; ++j)
+        for (int i = 0; i < s->nx; ++i) {
+            // src/wrappers.cuh:90-105
+            const double *q = (i < s->nx / 2) ? (j < s->ny / 2 ? U2 : U3) : (j < s->ny / 2 ? U1 : U4);
+            std::memcpy(&cells[((size_t)j * s->nx + i) * 4], q, 4 * sizeof(double));
+        }
+    return upload(s, cells.data(), 4);
+}
+
+int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride)
+{
+    if (int rc = check(s)) return rc;
+    if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
+    if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    soa_to_aos<<<148 * 4, 256, 0, s->stream>>>(s->U, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    CK(cudaGetLastError());
+    const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
+    const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(cells, s->scratch, bytes, kind, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FVM2D_OK;
+}
+
+int fvm2d_solve(fvm2d_solver *s)
+{
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    StepControl *c = s->ctl_h;
+    std::memset(c, 0, sizeof(StepControl));
+    c->step_limit = INT_MAX;
+    if (int rc = s->upload_control()) return rc;
+    const LaunchConfig cfg = s->config();
+    CK(kVariants[s->precision].init(cfg, s->stream));
+    s->need_init = false;
+    if (int rc = s->loop()) return rc;
+    s->total_steps += c->steps;
+    return FVM2D_OK;
+}
+
+int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done)
+{
+    if (steps_done) *steps_done = 0;
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (nsteps < 0) return fail(FVM2D_ERR_INVALID, "nsteps must be non-negative");
+    StepControl *c = s->ctl_h;
+    const int before = c->steps;
+    c->step_limit = (before > INT_MAX - nsteps) ? INT_MAX : before + nsteps;
+    c->done = 0;
+    c->active = 0;
+    if (int rc = s->upload_control()) return rc;
+    const LaunchConfig cfg = s->config();
+    if (s->need_init) {
+        CK(kVariants[s->precision].init(cfg, s->stream));
+        s->need_init = false;
+    } else {
+        CK(kVariants[s->precision].plan(cfg, s->stream));
+    }
+    if (int rc = s->loop()) return rc;
+    s->total_steps += c->steps - before;
+    if (steps_done) *steps_done = c->steps - before;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_computation_time_ms(fvm2d_solver *s, double *ms)
+{
+    if (int rc = check(s)) return rc;
+    if (!ms) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    *ms = s->last_ms;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_time_stages_count(fvm2d_solver *s, long long *count)
+{
+    if (int rc = check(s)) return rc;
+    if (!count) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    *count = s->total_steps;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_time(fvm2d_solver *s, double *t, int *steps, double *last_dt)
+{
+    if (int rc = check(s)) return rc;
+    if (t) *t = s->ctl_h->t;
+    if (steps) *steps = s->ctl_h->steps;
+    if (last_dt) *last_dt = s->ctl_h->dt;
+    return FVM2D_OK;
+}
+
+#pragma GCC visibility pop
+} // extern "C"

@@ -1,0 +1,56 @@
+// fvm2d_control.h -- records shared by every build of the kernels and the host runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fvm2d {
+
+// Device-resident loop state, one per solver handle.  The kernels of a step
+// read the step size from it and the step's last kernel advances it, so the
+// time loop of src/wrappers.cuh:196-284 runs without a host round trip.
+struct StepControl {
+    double t;                      // committed simulation time
+    double dt;                     // step size of the step in flight
+    double smax_last;              // max wave speed of the committed state
+    unsigned long long smax_bits;  // running max (bit pattern of a non-negative double)
+    int steps;                     // committed steps
+    int step_limit;                // no step starts once `steps` reaches this
+    int active;                    // 1 while a step is in flight
+    int done;                      // 1 once the loop of wrappers.cuh:196 has ended
+    unsigned int ticket;           // last-block detection in grid reductions
+    int pad;
+};
+
+struct PlanParams {
+    double t_end;  // end time
+    double cfl;    // CFL number
+    double hmin;   // min(width/nx, height/ny), wrappers.cuh:202
+};
+
+// Everything one build of the kernels needs to enqueue a step.
+struct LaunchConfig {
+    int nx, ny, pitch;
+    long long plane;       // elements between field planes
+    void *U, *A, *B;       // state buffers: U holds the state, A and B are sweep scratch
+    StepControl *ctl;
+    double hx, hy;         // width/nx, height/ny
+    double rhx, rhy;       // 1.0/hx, 1.0/hy
+    double alpha, gamma;
+    int strategy;
+    PlanParams plan;
+};
+
+// The entry points each build of the kernels provides (namespaces fp64,
+// fp64_strict, ...).
+#define FVM2D_DECLARE_VARIANT(ns)                                              \
+    namespace ns {                                                             \
+    cudaError_t prepare();                                                     \
+    cudaError_t enqueue_init(const LaunchConfig &c, cudaStream_t s);           \
+    cudaError_t enqueue_plan(const LaunchConfig &c, cudaStream_t s);           \
+    cudaError_t enqueue_step(const LaunchConfig &c, cudaStream_t s);           \
+    }
+
+FVM2D_DECLARE_VARIANT(fp64)
+FVM2D_DECLARE_VARIANT(fp64_strict)
+
+} // namespace fvm2d

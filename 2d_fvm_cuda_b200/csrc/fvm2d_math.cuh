@@ -1,0 +1,210 @@
+// fvm2d_math.cuh -- per-cell and per-interface arithmetic of the split step.
+//
+// One sweep treats its direction as "normal" (n) and the other as
+// "tangential" (t): a cell is (rho, p, un, ut).  In an x-sweep un = u; in a
+// y-sweep un = v, exactly as the reference's anti-transposed copy swaps the
+// u and v slots (src/basicFuns.cuh:249-262).
+//
+// The functions below keep the reference's operation order: with FMA
+// contraction off (-fmad=false) an FP64 build rounds every operation in the
+// same order as the reference built the same way, so the two agree bit for
+// bit.  The product build contracts (the nvcc default, as the reference's own
+// build does) and is checked against the reference within a relative L1
+// tolerance.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+#ifndef FVM2D_VARIANT
+#error "define FVM2D_VARIANT (the namespace of this build of the kernels) first"
+#endif
+
+namespace fvm2d {
+namespace FVM2D_VARIANT {
+
+template <typename Real>
+struct Cell {
+    Real rho, p, un, ut;
+};
+
+template <typename Real>
+__device__ __forceinline__ Real rmin(Real a, Real b) { return (b < a) ? b : a; }
+template <typename Real>
+__device__ __forceinline__ Real rmax(Real a, Real b) { return (a < b) ? b : a; }
+
+// Generalized-minmod slope of one component from its left (m), centre (c)
+// and right (p) values.  src/basicFuns.cuh:49-68.
+template <typename Real>
+__device__ __forceinline__ Real limited_slope(Real m, Real c, Real p, Real rh, Real alpha)
+{
+    Real central = (p - m) * Real(0.5) * rh;
+    Real back = (c - m) * rh * alpha;
+    Real fwd = (p - c) * rh * alpha;
+    Real p13 = central * fwd, p23 = back * fwd;
+    if (p13 > Real(0) && p23 > Real(0)) {
+        Real sign = (central <= Real(0)) ? Real(-1) : Real(1);
+        return sign * rmin(fabs(central), rmin(fabs(back), fabs(fwd)));
+    }
+    return Real(0);
+}
+
+// Interface state W = (rho, p, un, ut, e) and its time derivative Wt.
+template <typename Real>
+struct Interface {
+    Real rho, p, un, ut, e;
+    Real rho_t, p_t, un_t, ut_t, e_t;
+};
+
+// Relaxation GRP at one interface from the left/right face states (L, R)
+// and the slopes of the two cells (sL, sR).  src/basicFuns.cuh:86-189.
+// The star-region coefficients k_l, k_r, d_l, d_r read the velocity before
+// it receives the star value (basicFuns.cuh:151-155 see the initial 0.0 of
+// basicFuns.cuh:110); the literal `u0` keeps that.
+template <typename Real>
+__device__ __forceinline__ Interface<Real> relaxation_grp(const Cell<Real> &L, const Cell<Real> &R,
+                                                          const Cell<Real> &sL, const Cell<Real> &sR,
+                                                          Real g)
+{
+    const Real rho_l = L.rho, pi_l = L.p, u_l = L.un, v_l = L.ut;
+    const Real rho_r = R.rho, pi_r = R.p, u_r = R.un, v_r = R.ut;
+    const Real rho_lx = sL.rho, pi_lx = sL.p, u_lx = sL.un, v_lx = sL.ut;
+    const Real rho_rx = sR.rho, pi_rx = sR.p, u_rx = sR.un, v_rx = sR.ut;
+    const Real one = Real(1), two = Real(2), half = Real(0.5), zero = Real(0);
+
+    Real e_l = pi_l / rho_l / (g - one);
+    Real e_r = pi_r / rho_r / (g - one);
+    Real e_lx = pi_lx / rho_l / (g - one) - pi_l * rho_lx / rho_l / rho_l / (g - one);
+    Real e_rx = pi_rx / rho_r / (g - one) - pi_r * rho_rx / rho_r / rho_r / (g - one);
+    Real c_lx = half * sqrt(g / pi_l / rho_l) * (pi_l * rho_lx + rho_l * pi_lx);
+    Real c_rx = half * sqrt(g / pi_r / rho_r) * (pi_r * rho_rx + rho_r * pi_rx);
+
+    Interface<Real> o;
+    Real c_l, c_r;
+    Real a_l = sqrt(g * pi_l / rho_l), a_r = sqrt(g * pi_r / rho_r);
+    Real kappa = (g + one) / two;
+    if (pi_r >= pi_l) {
+        c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) / rho_r / a_r + u_l - u_r));
+        c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) / c_l + u_l - u_r));
+    } else {
+        c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) / rho_l / a_l + u_l - u_r));
+        c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) / c_r + u_l - u_r));
+    }
+
+    if (u_l - c_l / rho_l >= zero) {
+        // the whole wave fan moves right: left state (basicFuns.cuh:129-137)
+        Real rho = rho_l, pi = pi_l, u = u_l;
+        o.rho = rho_l; o.p = pi_l; o.un = u_l; o.ut = v_l; o.e = e_l;
+        o.rho_t = -rho * u_lx - u * rho_lx;
+        o.un_t = -u * u_lx - pi_lx / rho;
+        o.e_t = -u * e_lx - pi / rho * u_lx;
+        o.ut_t = -u * v_lx;
+        o.p_t = -u * pi_lx - c_l * c_l / rho_l * u_lx;
+    } else if (u_r + c_r / rho_r <= zero) {
+        // the whole wave fan moves left: right state (basicFuns.cuh:138-146)
+        Real rho = rho_r, pi = pi_r, u = u_r;
+        o.rho = rho_r; o.p = pi_r; o.un = u_r; o.ut = v_r; o.e = e_r;
+        o.rho_t = -rho * u_rx - u * rho_rx;
+        o.un_t = -u * u_rx - pi_rx / rho;
+        o.e_t = -u * e_rx - pi / rho * u_rx;
+        o.ut_t = -u * v_rx;
+        o.p_t = -u * pi_rx - c_r * c_r / rho * u_rx;
+    } else {
+        // star region (basicFuns.cuh:147-186)
+        const Real u0 = zero;
+        Real u_m = (u_l * c_l + u_r * c_r + pi_l - pi_r) / (c_l + c_r);
+        Real pi_m = ((u_l - u_r) * c_l * c_r + c_l * pi_r + c_r * pi_l) / (c_l + c_r);
+        Real k_l = -pi_lx - c_l * u_lx + half * (u0 - u_l) * c_lx;
+        Real k_r = -pi_rx + c_r * u_rx - half * (u0 - u_r) * c_rx;
+        Real d_l = Real(-2.0) * c_l * c_l / rho_l * u_lx - two * c_l / rho_l * pi_lx + c_l / rho_l * (u0 - u_l) * c_lx;
+        Real d_r = two * c_r * c_r / rho_r * u_rx - two * c_r / rho_r * pi_rx + c_r / rho_r * (u_r - u0) * c_rx;
+        Real Dpi_Dt = (c_r * d_l - c_l * d_r) / two / (c_l + c_r);
+        Real pi = pi_m, u = u_m, rho, e;
+        o.p = pi_m;
+        o.un = u_m;
+        if (u <= zero) {
+            Real rho_mr = c_r / (u_r - u_m + c_r / rho_r);
+            Real e_mr = e_r + (pi_m - pi_r) * (pi_m + pi_r) / two / c_r / c_r;
+            rho = rho_mr;
+            e = e_mr;
+            o.ut = v_r;
+            o.rho_t = -u * rho * rho * rho / (rho_r * c_r * c_r) * (c_r * c_r / rho_r / rho_r * rho_rx - c_r * u_rx + Real(1.5) * (u - u_r) * c_rx) + rho * rho * rho / (c_r * c_r * c_r) * (u + c_r / rho) * Dpi_Dt;
+            o.p_t = one / (c_l + c_r) * (c_l * c_r / rho_l * (one + u * rho / c_r) * k_l - c_l * c_r / rho_r * (one - u * rho / c_l) * k_r);
+            o.un_t = one / (c_l + c_r) * (c_l / rho_l * (one + u * rho / c_r) * k_l + c_r / rho_r * (one - u * rho * c_l / c_r / c_r) * k_r);
+            o.e_t = -u * rho / rho_r / c_r / c_r / c_r * (-pi_r * c_r * pi_rx + c_r * c_r * c_r * e_rx + two * (e_r - e) * c_r * c_r * c_rx) + pi / c_r / c_r * o.p_t;
+            Real v_x = rho / rho_r * v_rx;
+            o.ut_t = -u * v_x;
+        } else {
+            Real rho_ml = c_l / (u_m - u_l + c_l / rho_l);
+            Real e_ml = e_l + (pi_m - pi_l) * (pi_m + pi_l) / two / c_l / c_l;
+            rho = rho_ml;
+            e = e_ml;
+            o.ut = v_l;
+            o.rho_t = -u * rho * rho * rho / (rho_l * c_l * c_l) * (c_l * c_l / rho_l / rho_l * rho_lx + c_l * u_lx + Real(1.5) * (u - u_l) * c_lx) - rho * rho * rho / (c_l * c_l * c_l) * (u - c_l / rho) * Dpi_Dt;
+            o.p_t = one / (c_l + c_r) * (c_l * c_r / rho_l * (one + u * rho / c_r) * k_l - c_l * c_r / rho_r * (one - u * rho / c_l) * k_r);
+            o.un_t = one / (c_l + c_r) * (c_l / rho_l * (one + u * rho * c_r / c_l / c_l) * k_l + c_r / rho_r * (one - u * rho / c_l) * k_r);
+            o.e_t = -u * rho / rho_l / c_l / c_l / c_l * (-pi_l * c_l * pi_lx + c_l * c_l * c_l * e_lx + two * (e_l - e) * c_l * c_l * c_lx) + pi / c_l / c_l * o.p_t;
+            Real v_x = rho / rho_l * v_lx;
+            o.ut_t = -u * v_x;
+        }
+        o.rho = rho;
+        o.e = e;
+    }
+    return o;
+}
+
+// Midpoint flux F(W) + k/2 dF/dt in the sweep's conserved ordering
+// (mass, normal momentum, energy, tangential momentum).
+// src/basicFuns.cuh:14-34.
+template <typename Real>
+__device__ __forceinline__ Cell<Real> midpoint_flux(const Interface<Real> &w, Real k)
+{
+    const Real rho = w.rho, pi = w.p, u = w.un, v = w.ut, e = w.e;
+    const Real rho_t = w.rho_t, pi_t = w.p_t, u_t = w.un_t, v_t = w.ut_t, e_t = w.e_t;
+    const Real two = Real(2);
+    Cell<Real> F;
+    F.rho = rho * u + k / two * (rho * u_t + u * rho_t);
+    F.p = rho * u * u + pi + k / two * (rho_t * u * u + two * rho * u * u_t + pi_t);
+    F.un = rho * u * (e + u * u / two + v * v / two) + pi * u + k / two * (rho_t * u * e + rho * u_t * e + rho * u * e_t + rho_t * u * u * u / two + Real(1.5) * rho * u * u * u_t + rho_t * u * v * v / two + rho * u * v * v_t + rho * u_t * v * v / two + pi_t * u + pi * u_t);
+    F.ut = rho * u * v + k / two * (rho * u_t * v + u * rho_t * v + u * rho * v_t);
+    return F;
+}
+
+// Conservative update of one cell, primitive in and out:
+// W = cons(U); W -= (F_R - F_L) * lambda; U = prim(W).
+// src/basicFuns.cuh:195-212, 240-244.  Field slots of the flux Cell are
+// (mass, normal momentum, energy, tangential momentum).
+template <typename Real>
+__device__ __forceinline__ Cell<Real> conservative_update(const Cell<Real> &U, const Cell<Real> &FL,
+                                                          const Cell<Real> &FR, Real lambda, Real g)
+{
+    const Real one = Real(1), two = Real(2);
+    Real m0 = U.rho;
+    Real m1 = U.rho * U.un;
+    Real m2 = U.p / (g - one) + U.rho * (U.un * U.un + U.ut * U.ut) / two;
+    Real m3 = U.rho * U.ut;
+    m0 = m0 - (FR.rho - FL.rho) * lambda;
+    m1 = m1 - (FR.p - FL.p) * lambda;
+    m2 = m2 - (FR.un - FL.un) * lambda;
+    m3 = m3 - (FR.ut - FL.ut) * lambda;
+    Cell<Real> o;
+    o.rho = m0;
+    o.p = (g - one) * (m2 - m1 * m1 / m0 / two - m3 * m3 / m0 / two);
+    o.un = m1 / m0;
+    o.ut = m3 / m0;
+    return o;
+}
+
+// |(u, v)| + sqrt(gamma p / rho) in the array's own (u, v) order.
+// src/basicFuns.cuh:223-224.
+template <typename Real>
+__device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, double g)
+{
+    double du = double(u), dv = double(v);
+    double velo = sqrt(du * du + dv * dv);
+    double c = sqrt(g * double(p) / double(rho));
+    return fabs(velo) + c;
+}
+
+} // namespace FVM2D_VARIANT
+} // namespace fvm2d

@@ -1,0 +1,148 @@
+/*
+ * fvm2d.h -- C ABI of the B200 split 2D Euler solver (libfvm2d.so).
+ *
+ * The reference exposes one C++ class, RGRP_2D_CUDA, header-only in
+ * src/wrappers.cuh:26-65, with enum class ghostCellStrategy at
+ * src/wrappers.cuh:17-24.  Each entry point below replaces one of its
+ * members (cited), with plain pointers and sizes so any language can bind it.
+ * include/rgrp_2d_cuda.hpp rebuilds the reference's C++ class on top of this
+ * ABI for drop-in source compatibility.
+ *
+ * Conventions
+ *  - Every call returns an int status (FVM2D_OK on success) and never throws;
+ *    fvm2d_last_error() gives a message for the calling thread's last failure.
+ *  - A handle belongs to the CUDA device current when it was created and owns
+ *    one CUDA stream; it is not thread-safe.  All its calls return with their
+ *    device work finished (the solve is synchronous, as the reference's is).
+ *  - States are `ny` rows of `nx` cells, row-major, including the two ghost
+ *    layers on every side (src/wrappers.cuh:67-78).  A host cell is `stride`
+ *    doubles: stride 4 is (rho, p, u, v); stride 5 is the reference's vec5d
+ *    (src/ghostCellPresets.cuh:4-45), whose fifth slot is ignored on input
+ *    and written as 0 on output.  Pointers may be host (pageable or pinned)
+ *    or device memory.
+ *  - Axis convention (src/basicFuns.cuh:249-262): +u toward increasing column
+ *    i, +v toward decreasing row j.
+ */
+#ifndef FVM2D_H
+#define FVM2D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FVM2D_OK 0
+#define FVM2D_ERR_INVALID 1  /* bad argument or unsupported size */
+#define FVM2D_ERR_CUDA 2     /* a CUDA call failed (no device, out of memory, ...) */
+#define FVM2D_ERR_STATE 3    /* call out of order: no state uploaded yet */
+
+/* Ghost-cell strategies.  0..4 are ghostCellStrategy (src/wrappers.cuh:17-24)
+ * with the reference's dispatch (src/wrappers.cuh:265-280): REFLECTIVE and
+ * DOUBLE_MACH both run the double-Mach preset.  PERIODIC and REFLECTIVE_TB
+ * have no reference counterpart. */
+enum fvm2d_ghost_strategy {
+    FVM2D_OUTFLOW = 0,       /* src/ghostCellPresets.cuh:106-145 */
+    FVM2D_REFLECTIVE = 1,    /* src/ghostCellPresets.cuh:48-103 (as the reference dispatches it) */
+    FVM2D_JET = 2,           /* src/ghostCellPresets.cuh:148-193 */
+    FVM2D_JET800 = 3,        /* src/ghostCellPresets.cuh:196-241 */
+    FVM2D_DOUBLE_MACH = 4,   /* src/ghostCellPresets.cuh:48-103 */
+    FVM2D_PERIODIC = 5,      /* two-layer wrap in both directions */
+    FVM2D_REFLECTIVE_TB = 6  /* mirrored top/bottom rows with v negated, transmissive columns */
+};
+
+/* Arithmetic modes (no reference counterpart: the reference has one FP64 build). */
+enum fvm2d_precision {
+    FVM2D_FP64 = 0,        /* FP64, FMA contraction as nvcc does by default (the reference's build) */
+    FVM2D_FP64_STRICT = 1  /* FP64, no contraction: bit-exact with the reference built -fmad=false */
+};
+
+typedef struct fvm2d_solver fvm2d_solver;
+
+/* Message for the calling thread's last failed call ("" if none). */
+const char *fvm2d_last_error(void);
+
+/* Library version string. */
+const char *fvm2d_version(void);
+
+/* Creates a solver for an nx x ny array (ghosts included, nx, ny >= 6) on
+ * the current CUDA device.  Replaces RGRP_2D_CUDA(const vector<vector<vec5d>>&)
+ * (src/wrappers.cuh:67-78) together with fvm2d_set_state, and the sizes of
+ * setRPInitialData (src/wrappers.cuh:80-85).  Defaults as the reference
+ * (src/wrappers.cuh:49-52): width = height = 1, end time 0, CFL 0.5,
+ * alpha 1.9, gamma 1.4, outflow. */
+int fvm2d_create(fvm2d_solver **out, int nx, int ny);
+
+/* Releases the handle and its device memory.  Replaces the per-solve
+ * cudaFree calls and clear() (src/wrappers.cuh:292-303, 347-353). */
+int fvm2d_destroy(fvm2d_solver *s);
+
+/* setSpatialLayout (src/wrappers.cuh:110-114): extent of the whole array,
+ * ghosts included; h_x = width/nx, h_y = height/ny. */
+int fvm2d_set_spatial_layout(fvm2d_solver *s, double width, double height);
+
+/* setTimeLayout(endTime, CFL) (src/wrappers.cuh:116-120). */
+int fvm2d_set_time_layout(fvm2d_solver *s, double end_time, double cfl);
+
+/* setTimeLayout(endTime) (src/wrappers.cuh:122-125). */
+int fvm2d_set_end_time(fvm2d_solver *s, double end_time);
+
+/* setCFL (src/wrappers.cuh:127-130). */
+int fvm2d_set_cfl(fvm2d_solver *s, double cfl);
+
+/* setAlpha (src/wrappers.cuh:132-135): limiter parameter of the generalized minmod. */
+int fvm2d_set_alpha(fvm2d_solver *s, double alpha);
+
+/* setGamma (src/wrappers.cuh:137-140). */
+int fvm2d_set_gamma(fvm2d_solver *s, double gamma);
+
+/* setGhostCellStrategy (src/wrappers.cuh:142-145); strategy is an
+ * fvm2d_ghost_strategy value. */
+int fvm2d_set_ghost_strategy(fvm2d_solver *s, int strategy);
+
+/* Selects the arithmetic build (fvm2d_precision).  No reference counterpart. */
+int fvm2d_set_precision(fvm2d_solver *s, int precision);
+
+/* Uploads a state of ny x nx cells of `stride` doubles (4 or 5).  Replaces the
+ * constructor's copy of U0 (src/wrappers.cuh:67-78) and the H2D copy in
+ * solve() (src/wrappers.cuh:185).  Resets time and step counters of the
+ * current run to zero. */
+int fvm2d_set_state(fvm2d_solver *s, const double *cells, int stride);
+
+/* setRPInitialData (src/wrappers.cuh:80-108): four constant states (4 doubles
+ * each: rho, p, u, v) split at column nx/2 and row ny/2 -- U2 | U1 over U3 | U4. */
+int fvm2d_set_rp_initial_data(fvm2d_solver *s, const double *U1, const double *U2,
+                              const double *U3, const double *U4);
+
+/* Downloads the current state into ny x nx cells of `stride` doubles.
+ * Replaces the D2H copy and result of solve() (src/wrappers.cuh:290-305). */
+int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride);
+
+/* solve() (src/wrappers.cuh:154-306): runs the time loop from t = 0 on the
+ * current state until the end time (or the step-size guard of
+ * src/wrappers.cuh:204-207).  The result stays in the handle; like the
+ * reference, a second call starts again from t = 0 on the previous result. */
+int fvm2d_solve(fvm2d_solver *s);
+
+/* Advances the current run by at most nsteps steps from its current time,
+ * stopping early at the end time.  *steps_done (may be NULL) receives the
+ * steps taken.  No reference counterpart (step granularity for checks and
+ * benchmarks). */
+int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done);
+
+/* getComputationTime_ms (src/wrappers.cuh:308-311): wall time of the last
+ * solve()/advance() loop in milliseconds. */
+int fvm2d_get_computation_time_ms(fvm2d_solver *s, double *ms);
+
+/* getTimeStagesCount (src/wrappers.cuh:313-316): steps taken by all solve()
+ * and advance() calls since the handle was created (the reference never
+ * resets its counter either, src/wrappers.cuh:252). */
+int fvm2d_get_time_stages_count(fvm2d_solver *s, long long *count);
+
+/* Time and step count of the current run (no reference counterpart; the
+ * reference keeps them in solve()'s locals, src/wrappers.cuh:191-196). */
+int fvm2d_get_time(fvm2d_solver *s, double *t, int *steps, double *last_dt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FVM2D_H */

@@ -1,0 +1,218 @@
+"""GPU parity: libfvm2d.so (through its C ABI) against the oracle and the
+reference's own builds.
+
+* FP64_STRICT (no FMA contraction) must equal the oracle bit for bit, step by
+  step, on every ghost-cell preset, odd sizes included.
+* FP64 (contraction on, the product default) must stay within a relative L1
+  of 1e-10 per field of the oracle at the final time of the 400x400
+  four-quadrant workload (620 steps).
+* The reference's CUDA kernels (oracle/_ref/ref_gpu*) on the same GPU: the
+  -fmad=false build equals FP64_STRICT bit for bit; the default build is
+  within the same 1e-10 relative L1 of FP64.
+* At 4096^2, where the oracle is too slow, size-independent properties: the
+  step commutes with the reference's anti-transpose (x<->y with u<->v), and
+  periodic runs conserve mass and momentum.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import REF_GPU, REF_GPU_NOFMA, run_ref_gpu
+
+pytestmark = pytest.mark.gpu
+
+REL_L1_TOL = 1e-10  # relative L1 per field at the final time, FMA build vs reference
+RUN_KEYS = ("width", "height", "cfl", "alpha", "gamma", "t_end", "strategy")
+
+
+def gpu_run(pkg, U0, max_steps=None, precision=0, **kw):
+    ny, nx = U0.shape[:2]
+    h = pkg.Handle(nx, ny)
+    try:
+        h.configure(kw.get("width", 1.0), kw.get("height", 1.0), kw.get("t_end", 0.0), kw.get("cfl", 0.5),
+                    kw.get("alpha", 1.9), kw.get("gamma", 1.4), kw.get("strategy", 0), precision)
+        h.set_state(U0)
+        if max_steps is None or max_steps < 0:
+            h.solve()
+        else:
+            h.advance(max_steps)
+        U = h.get_state(4)
+        t, steps, _ = h.time()
+        return U, steps, t
+    finally:
+        h.close()
+
+
+def rel_l1(A, B):
+    return [np.abs(A[..., f] - B[..., f]).sum() / np.abs(B[..., f]).sum() for f in range(4)]
+
+
+def anti_transpose(U):
+    """src/basicFuns.cuh:249-262: out[(nx-1-x), (ny-1-y)] = in[y, x] with u<->v."""
+    V = U[::-1, ::-1].transpose(1, 0, 2).copy()
+    V[..., [2, 3]] = V[..., [3, 2]]
+    return V
+
+
+@pytest.mark.parametrize("strategy", range(7))
+@pytest.mark.parametrize("shape", [(32, 48), (29, 37)])
+def test_strict_equals_oracle_every_step(pkg, oracle, strategy, shape):
+    ny, nx = shape
+    U = pkg.scenarios.seeded_four_quadrant(nx, ny, 1000 + strategy)
+    if strategy in (5, 6):  # the new presets need a consistent ring first
+        U = oracle.ghost(U, strategy, 0.0, 1.0, 1.0)
+    kw = dict(width=1.0, height=0.8, cfl=0.45, alpha=1.9, gamma=1.4, t_end=1.0, strategy=strategy)
+    h = pkg.Handle(nx, ny)
+    h.configure(kw["width"], kw["height"], kw["t_end"], kw["cfl"], kw["alpha"], kw["gamma"], strategy, pkg.FP64_STRICT)
+    h.set_state(U)
+    t = 0.0
+    for k in range(8):
+        r = oracle.step(U, t=t, **kw)
+        assert r is not None
+        U, t, dt = r
+        assert h.advance(1) == 1
+        tg, sg, dtg = h.time()
+        assert (tg, sg, dtg) == (t, k + 1, dt)
+        G = h.get_state(4)
+        assert np.array_equal(G, U, equal_nan=True), f"step {k}: max |diff| {np.nanmax(np.abs(G - U))}"
+    h.close()
+
+
+@pytest.mark.parametrize("name", ["quad_outflow_48x32", "quad_reflective_32x48", "quad_outflow_alpha1_64x64",
+                                  "double_mach_16", "jet_32", "jet800_16", "four_shocks_64", "four_contacts_48",
+                                  "sedov_32", "quad_gamma5_3_32x32"])
+def test_strict_equals_reference_fixture(pkg, golden, name):
+    z, manifest = golden
+    m = manifest[name]
+    U, steps, t = gpu_run(pkg, z[f"{name}/U0"], max_steps=m["max_steps"], precision=pkg.FP64_STRICT,
+                          **{k: m[k] for k in RUN_KEYS})
+    assert (steps, t) == (m["steps"], m["t"])
+    assert np.array_equal(U, z[f"{name}/U1"], equal_nan=True)
+
+
+def test_fma_within_tolerance_full_quadrant_workload(pkg, oracle, golden):
+    """400x400 incl. ghosts, [0,1]^2, gamma 1.4, outflow, CFL 0.45, t_end 0.2, alpha 1.9, seed 0."""
+    z, manifest = golden
+    m = manifest["quad_outflow_400x400_seed0"]
+    kw = {k: m[k] for k in RUN_KEYS}
+    U0 = pkg.scenarios.seeded_four_quadrant(m["nx"], m["ny"], m["seed"])
+    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64, **kw)
+    assert steps == m["steps"] and t == pytest.approx(m["t"], rel=0, abs=1e-15)
+    O, osteps, ot = oracle.solve(U0, **kw)
+    assert osteps == steps
+    err = rel_l1(G, O)
+    assert max(err) <= REL_L1_TOL, err
+    S, ssteps, st = gpu_run(pkg, U0, precision=pkg.FP64_STRICT, **kw)
+    assert (ssteps, st) == (osteps, ot) and np.array_equal(S, O)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU_NOFMA), reason="reference CUDA build not present")
+def test_reference_cuda_nofma_equals_strict(pkg):
+    U0 = pkg.scenarios.seeded_four_quadrant(96, 64, 77)
+    kw = dict(width=1.5, height=1.0, cfl=0.45, alpha=1.9, gamma=1.4, t_end=0.05, strategy=0)
+    R, rsteps, rt, _, _ = run_ref_gpu(U0, fma=False, **kw)
+    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64_STRICT, **kw)
+    assert (steps, t) == (rsteps, rt)
+    assert np.array_equal(G, R)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA build not present")
+@pytest.mark.parametrize("strategy", [0, 4])
+def test_reference_cuda_default_build_within_tolerance(pkg, golden, strategy):
+    z, manifest = golden
+    m = manifest["quad_outflow_400x400_seed0"]
+    kw = {k: m[k] for k in RUN_KEYS}
+    kw["strategy"] = strategy
+    U0 = pkg.scenarios.seeded_four_quadrant(400, 400, m["seed"])
+    R, rsteps, rt, _, _ = run_ref_gpu(U0, fma=True, **kw)
+    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64, **kw)
+    assert steps == rsteps
+    err = rel_l1(G, R)
+    assert max(err) <= REL_L1_TOL, err
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_full_size_step_commutes_with_anti_transpose(pkg, precision):
+    """S(rot U) = rot S(U) at 4096^2: checks the reversed-direction y-sweep
+    against the x-sweep on the whole headline-size array."""
+    n = 4096
+    U0 = pkg.scenarios.seeded_four_quadrant(n, n, 4242)
+    kw = dict(width=1.0, height=1.0, cfl=0.45, alpha=1.9, gamma=1.4, t_end=1.0, strategy=0)
+    A, sa, ta = gpu_run(pkg, U0, max_steps=3, precision=precision, **kw)
+    B, sb, tb = gpu_run(pkg, anti_transpose(U0), max_steps=3, precision=precision, **kw)
+    assert sa == sb == 3
+    if precision == pkg.FP64_STRICT:
+        assert ta == tb
+        assert np.array_equal(anti_transpose(A), B)
+    else:  # the wave-speed sum u*u + v*v may contract differently for (u, v) and (v, u)
+        assert ta == pytest.approx(tb, rel=1e-14)
+        assert max(rel_l1(anti_transpose(A), B)) < 1e-12
+
+
+def test_full_size_periodic_conservation(pkg, oracle):
+    """Periodic 4096^2: interior totals of mass and momentum are conserved."""
+    n = 4096
+    rng = np.random.default_rng(5)
+    y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    U0 = np.empty((n, n, 4))
+    U0[..., 0] = 1.0 + 0.2 * np.sin(2 * np.pi * 3 * x / (n - 4)) * np.cos(2 * np.pi * 2 * y / (n - 4))
+    U0[..., 1] = 1.0 + 0.1 * rng.random()
+    U0[..., 2] = 0.5
+    U0[..., 3] = -0.25
+    U0 = oracle.ghost(U0, 5)
+    kw = dict(width=1.0, height=1.0, cfl=0.45, alpha=1.9, gamma=1.4, t_end=1.0, strategy=5)
+    G, steps, _ = gpu_run(pkg, U0, max_steps=4, precision=pkg.FP64, **kw)
+    assert steps == 4
+    inner = (slice(2, n - 2), slice(2, n - 2))
+
+    def totals(U):
+        r = U[inner][..., 0]
+        return np.array([r.sum(), (r * U[inner][..., 2]).sum(), (r * U[inner][..., 3]).sum()])
+
+    a, b = totals(U0), totals(G)
+    assert np.all(np.abs(b - a) <= 1e-11 * np.abs(a).max())
+
+
+def test_solve_api_behaves_like_the_reference(pkg):
+    """RGRP_2D_CUDA mirror: solve() twice restarts from t = 0 on the previous
+    result and the stage counter accumulates (src/wrappers.cuh:252,290)."""
+    s = pkg.RGRP_2D_CUDA()
+    s.setRPInitialData((1.5, 1.5, 0, 0, 0), (0.5323, 0.3, 1.206, 0, 0), (0.138, 0.029, 1.206, 1.206, 0),
+                       (0.5323, 0.3, 0, 1.206, 0), 64, 48)
+    s.setSpatialLayout(1.0, 0.75)
+    s.setTimeLayout(0.02, 0.5)
+    s.setAlpha(2.0)
+    s.setGhostCellStrategy(pkg.ghostCellStrategy.outflow)
+    U1 = s.solve()
+    n1 = s.getTimeStagesCount()
+    assert U1.shape == (48, 64, 5) and np.all(U1[..., 4] == 0) and n1 > 0
+    assert s.getComputationTime_ms() > 0
+    U2 = s.solve()
+    assert s.getTimeStagesCount() > n1
+    assert not np.array_equal(U1, U2)
+
+
+def test_device_pointer_state_io(pkg):
+    torch = pytest.importorskip("torch")
+    U0 = pkg.scenarios.seeded_four_quadrant(40, 30, 9)
+    h = pkg.Handle(40, 30)
+    h.configure(t_end=0.01, cfl=0.45)
+    d = torch.from_numpy(np.ascontiguousarray(U0)).cuda()
+    h.set_state_ptr(d.data_ptr(), 4)
+    h.advance(2)
+    out = torch.empty_like(d)
+    h.get_state_ptr(out.data_ptr(), 4)
+    torch.cuda.synchronize()
+    ref = h.get_state(4)
+    assert np.array_equal(out.cpu().numpy(), ref)
+    h.close()
+
+
+def test_invalid_calls_return_errors(pkg):
+    h = pkg.Handle(16, 16)
+    with pytest.raises(pkg.FVM2DError):
+        h.configure(strategy=42)
+    with pytest.raises(pkg.FVM2DError):
+        h.solve()  # no state yet
+    h.close()
