@@ -42,6 +42,8 @@ SIGNATURES = [
     ("fvm2d_get_computation_time_ms", ctypes.c_int, [_vp, _dp]),
     ("fvm2d_get_time_stages_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
+    ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
 ]
 
 _LIB = None
@@ -154,6 +156,21 @@ class Handle:
         ms = ctypes.c_double(0)
         check(self.lib.fvm2d_get_computation_time_ms(self.h, ctypes.byref(ms)))
         return ms.value
+
+    def run_stats(self):
+        """(device_ms, kernel_launches) of the last solve()/advance() loop."""
+        ms = ctypes.c_double(0)
+        n = ctypes.c_longlong(0)
+        check(self.lib.fvm2d_get_run_stats(self.h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def profile_kernels(self, nsteps: int):
+        """Mean per-kernel times (ms) over up to nsteps steps: [sweep X, sweep Y,
+        sweep Y, sweep X + average, ghost ring], and the steps taken."""
+        out = (ctypes.c_double * 5)()
+        k = ctypes.c_int(0)
+        check(self.lib.fvm2d_profile_kernels(self.h, int(nsteps), out, ctypes.byref(k)))
+        return list(out), k.value
 
     def time_stages_count(self) -> int:
         c = ctypes.c_longlong(0)

@@ -6,9 +6,9 @@
 //   scratch  two more state-sized buffers (A, B) that the sweeps write, also
 //            used as the staging area for uploads and downloads;
 //   ctl      the device-resident StepControl of the time loop;
-//   a CUDA graph of GRAPH_STEPS steps (5 kernels each) replayed until the
-//   control record says the loop has ended, so the only host round trip is
-//   one 64-byte read per graph replay (the reference reads the max wave
+//   CUDA graphs of 16 steps and of 1 step (5 kernels each) replayed until
+//   the control record says the loop has ended, so the only host round trip
+//   is one 64-byte read per graph replay (the reference reads the max wave
 //   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
 #include "../../include/fvm2d.h"
 #include "fvm2d_control.h"
@@ -49,7 +49,7 @@ struct Variant {
     cudaError_t (*prepare)();
     cudaError_t (*init)(const LaunchConfig &, cudaStream_t);
     cudaError_t (*plan)(const LaunchConfig &, cudaStream_t);
-    cudaError_t (*step)(const LaunchConfig &, cudaStream_t);
+    cudaError_t (*step)(const LaunchConfig &, cudaStream_t, cudaEvent_t *);
 };
 
 const Variant kVariants[] = {
@@ -107,13 +107,18 @@ struct fvm2d_solver {
     double *scratch = nullptr;  // A then B
     StepControl *ctl = nullptr;
     StepControl *ctl_h = nullptr;  // pinned mirror
-    cudaGraphExec_t graph = nullptr;
+    // replayed graphs: kGraphSteps[g] steps each; built on first use for the
+    // current precision and parameters, dropped by every setter
+    static constexpr int kGraphSteps[2] = {16, 1};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_variant = -1;
-    int graph_steps = 16;
     bool have_state = false;
     bool need_init = true;
-    double last_ms = 0.0;
+    double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
+    double last_device_ms = 0.0;  // CUDA-event time of the last loop on the stream
+    long long last_launches = 0;  // kernels launched by the last loop
     long long total_steps = 0;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
 
     LaunchConfig config() const
     {
@@ -141,51 +146,69 @@ struct fvm2d_solver {
 
     void drop_graph()
     {
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
+        for (auto &g : graph) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
         graph_variant = -1;
     }
 
-    int build_graph()
+    int build_graphs()
     {
-        if (graph && graph_variant == precision) return FVM2D_OK;
+        if (graph_variant == precision && graph[0] && graph[1]) return FVM2D_OK;
         drop_graph();
         const LaunchConfig c = config();
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = cudaSuccess;
-        for (int k = 0; k < graph_steps && e == cudaSuccess; ++k) e = kVariants[precision].step(c, stream);
-        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
-        if (e != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return cuda_fail(e, "capture of the step kernels");
-        }
-        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            graph = nullptr;
-            return cuda_fail(e, "cudaGraphInstantiate");
+        for (int which = 0; which < 2; ++which) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = cudaSuccess;
+            for (int k = 0; k < kGraphSteps[which] && e == cudaSuccess; ++k)
+                e = kVariants[precision].step(c, stream, nullptr);
+            cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+            if (e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return cuda_fail(e, "capture of the step kernels");
+            }
+            if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&graph[which], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                graph[which] = nullptr;
+                return cuda_fail(e, "cudaGraphInstantiate");
+            }
         }
         graph_variant = precision;
         return FVM2D_OK;
     }
 
-    // Replays the step graph until the control record says no step is in
-    // flight.  The record on the device must already be planned.
-    int loop()
+    // Replays the step graphs until the control record says no step is in
+    // flight.  The record on the device must already be planned; `first`
+    // kernels (init or plan) were enqueued just before.
+    // `budget` bounds the steps this loop may start; the long graph is
+    // replayed while at least its length remains, then the one-step graph.
+    int loop(int first, long long budget)
     {
-        int rc = build_graph();
+        int rc = build_graphs();
         if (rc) return rc;
         auto t0 = std::chrono::high_resolution_clock::now();
+        long long launches = first;
         for (;;) {
-            CK(cudaGraphLaunch(graph, stream));
+            const int which = budget >= kGraphSteps[0] ? 0 : 1;
+            CK(cudaGraphLaunch(graph[which], stream));
+            budget -= kGraphSteps[which];
+            launches += (long long)kGraphSteps[which] * fvm2d::kStepKernels;
             CK(cudaMemcpyAsync(ctl_h, ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, stream));
             CK(cudaStreamSynchronize(stream));
             if (!ctl_h->active) break;
         }
+        CK(cudaEventRecord(ev_end, stream));
+        CK(cudaEventSynchronize(ev_end));
         auto t1 = std::chrono::high_resolution_clock::now();
         last_ms = std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count() / 1000.0;
+        float dms = 0.f;
+        CK(cudaEventElapsedTime(&dms, ev_begin, ev_end));
+        last_device_ms = dms;
+        last_launches = launches;
         return FVM2D_OK;
     }
 
@@ -257,6 +280,7 @@ int fvm2d_create(fvm2d_solver **out, int nx, int ny)
         if ((e = cudaMalloc(&s->scratch, 2 * state_bytes))) { rc = cuda_fail(e, "cudaMalloc(scratch)"); break; }
         if ((e = cudaMalloc(&s->ctl, sizeof(StepControl)))) { rc = cuda_fail(e, "cudaMalloc(control)"); break; }
         if ((e = cudaMallocHost(&s->ctl_h, sizeof(StepControl)))) { rc = cuda_fail(e, "cudaMallocHost"); break; }
+        if ((e = cudaEventCreate(&s->ev_begin)) || (e = cudaEventCreate(&s->ev_end))) { rc = cuda_fail(e, "cudaEventCreate"); break; }
         std::memset(s->ctl_h, 0, sizeof(StepControl));
         if ((e = cudaMemsetAsync(s->U, 0, state_bytes, s->stream))) { rc = cuda_fail(e, "cudaMemset"); break; }
         if ((e = cudaMemsetAsync(s->scratch, 0, 2 * state_bytes, s->stream))) { rc = cuda_fail(e, "cudaMemset"); break; }
@@ -281,6 +305,8 @@ int fvm2d_destroy(fvm2d_solver *s)
     if (s->scratch) cudaFree(s->scratch);
     if (s->ctl) cudaFree(s->ctl);
     if (s->ctl_h) cudaFreeHost(s->ctl_h);
+    if (s->ev_begin) cudaEventDestroy(s->ev_begin);
+    if (s->ev_end) cudaEventDestroy(s->ev_end);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FVM2D_OK;
@@ -372,9 +398,11 @@ int fvm2d_solve(fvm2d_solver *s)
     c->step_limit = INT_MAX;
     if (int rc = s->upload_control()) return rc;
     const LaunchConfig cfg = s->config();
+    if (int rc = s->build_graphs()) return rc;
+    CK(cudaEventRecord(s->ev_begin, s->stream));
     CK(kVariants[s->precision].init(cfg, s->stream));
     s->need_init = false;
-    if (int rc = s->loop()) return rc;
+    if (int rc = s->loop(1, LLONG_MAX)) return rc;
     s->total_steps += c->steps;
     return FVM2D_OK;
 }
@@ -392,13 +420,15 @@ int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done)
     c->active = 0;
     if (int rc = s->upload_control()) return rc;
     const LaunchConfig cfg = s->config();
+    if (int rc = s->build_graphs()) return rc;
+    CK(cudaEventRecord(s->ev_begin, s->stream));
     if (s->need_init) {
         CK(kVariants[s->precision].init(cfg, s->stream));
         s->need_init = false;
     } else {
         CK(kVariants[s->precision].plan(cfg, s->stream));
     }
-    if (int rc = s->loop()) return rc;
+    if (int rc = s->loop(1, nsteps)) return rc;
     s->total_steps += c->steps - before;
     if (steps_done) *steps_done = c->steps - before;
     return FVM2D_OK;
@@ -426,6 +456,55 @@ int fvm2d_get_time(fvm2d_solver *s, double *t, int *steps, double *last_dt)
     if (t) *t = s->ctl_h->t;
     if (steps) *steps = s->ctl_h->steps;
     if (last_dt) *last_dt = s->ctl_h->dt;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_launches)
+{
+    if (int rc = check(s)) return rc;
+    if (device_ms) *device_ms = s->last_device_ms;
+    if (kernel_launches) *kernel_launches = s->last_launches;
+    return FVM2D_OK;
+}
+
+int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done)
+{
+    if (steps_done) *steps_done = 0;
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (nsteps < 1 || !kernel_ms) return fail(FVM2D_ERR_INVALID, "nsteps must be positive and kernel_ms non-null");
+    cudaEvent_t ev[fvm2d::kStepKernels + 1] = {};
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    double acc[fvm2d::kStepKernels] = {};
+    int done = 0, rc = FVM2D_OK;
+    StepControl *c = s->ctl_h;
+    const LaunchConfig cfg = s->config();
+    for (int k = 0; k < nsteps && rc == FVM2D_OK; ++k) {
+        const int before = c->steps;
+        c->step_limit = before + 1;
+        c->done = 0;
+        c->active = 0;
+        cudaError_t e;
+        if ((rc = s->upload_control())) break;
+        e = s->need_init ? kVariants[s->precision].init(cfg, s->stream) : kVariants[s->precision].plan(cfg, s->stream);
+        s->need_init = false;
+        if (!e) e = kVariants[s->precision].step(cfg, s->stream, ev);
+        if (!e) e = cudaMemcpyAsync(c, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream);
+        if (!e) e = cudaStreamSynchronize(s->stream);
+        if (e) { rc = cuda_fail(e, "profiled step"); break; }
+        if (c->steps == before) break;  // the loop has ended: nothing ran
+        ++done;
+        for (int q = 0; q < fvm2d::kStepKernels; ++q) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
+            acc[q] += ms;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    s->total_steps += done;
+    for (int q = 0; q < fvm2d::kStepKernels; ++q) kernel_ms[q] = done ? acc[q] / done : 0.0;
+    if (steps_done) *steps_done = done;
     return FVM2D_OK;
 }
 

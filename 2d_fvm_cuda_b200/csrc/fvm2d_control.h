@@ -40,6 +40,9 @@ struct LaunchConfig {
     PlanParams plan;
 };
 
+// Kernels per step: sweep X, sweep Y, sweep Y, sweep X + average, ghost ring.
+constexpr int kStepKernels = 5;
+
 // The entry points each build of the kernels provides (namespaces fp64,
 // fp64_strict, ...).
 #define FVM2D_DECLARE_VARIANT(ns)                                              \
@@ -47,7 +50,7 @@ struct LaunchConfig {
     cudaError_t prepare();                                                     \
     cudaError_t enqueue_init(const LaunchConfig &c, cudaStream_t s);           \
     cudaError_t enqueue_plan(const LaunchConfig &c, cudaStream_t s);           \
-    cudaError_t enqueue_step(const LaunchConfig &c, cudaStream_t s);           \
+    cudaError_t enqueue_step(const LaunchConfig &c, cudaStream_t s, cudaEvent_t *ev); \
     }
 
 FVM2D_DECLARE_VARIANT(fp64)

@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Throughput of the split 2D Euler step on B200: one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+
+Workload: the seeded four-quadrant Riemann problem (rho~U[0.1,2],
+p~U[0.02,2], u,v~U[-1.5,1.5], seed = rank) on a 4096 x 4096 array including
+ghosts, [0,1]^2, gamma 1.4, CFL 0.45, alpha 1.9, transmissive ghosts, FP64.
+A step is one full split step  U <- ghost((Y(X(U)) + X(Y(U)))/2)  of the
+whole array; cell-updates/s counts all nx*ny cells per step.
+
+product arm (default):
+  value       device-resident: K steps through fvm2d_advance, timed with CUDA
+              events on the solver's stream (max over ranks), state buffers
+              3 x 537 MB, far above the 126 MB L2
+  e2e         the public C ABI with host buffers: the initial state uploaded
+              from pinned host memory, then every step one fvm2d_advance(1)
+              call that reads the step's control record (t, dt, step count)
+              back to the host, then the final state downloaded to pinned
+              host memory -- all inside the timed region
+  roofline    the dominant kernel's algorithmic bytes / its mean CUDA-event
+              duration against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own kernels compiled for the host
+              (oracle/_ref/libref_host.so) on all host cores, bounded sample
+  reference_cuda  the reference's own CUDA kernels (oracle/_ref/ref_gpu) on
+              the same GPU and workload, timed by its own loop timer
+N > 1: independent replicas, one per GPU (the four-quadrant problems share
+nothing), weak scaling, max-over-ranks device time.
+
+reference arm (--impl reference): rank 0 times the reference's own kernels
+on the host cores (oracle/_ref/libref_host.so; the C oracle if that build is
+absent) with every host thread, each step a 1024 x 1024 sample of the same
+workload; other ranks exit at once.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s FP64 & FP32 vs HBM roofline at stated L1 error; adjoint/fwd ratio"
+UNIT = "cell-updates/s"
+N_CELLS = 4096
+CFG = dict(width=1.0, height=1.0, t_end=0.2, cfl=0.45, alpha=1.9, gamma=1.4, strategy=0)
+CPU_SAMPLE_N = 1024
+FALLBACK_HBM_GBS = 6650.0
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup(world, local_rank):
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local_rank))
+    return dist
+
+
+def allreduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference_rate(pkg, seconds: float = 12.0, max_steps: int = 60):
+    """Reference kernels on the host cores: cell-updates/s on a 1024^2 sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, RefHost
+    threads = os.cpu_count() or 1
+    U = pkg.scenarios.seeded_four_quadrant(CPU_SAMPLE_N, CPU_SAMPLE_N, 0)
+    kw = {k: v for k, v in CFG.items()}
+    if RefHost.available():
+        ref, kind = RefHost(threads=threads), "reference"
+        one = lambda U, t: ref.run(U, t0=t, max_steps=1, **kw)  # noqa: E731
+    else:
+        orc, kind = Oracle(threads=threads), "port"
+
+        def one(U, t):
+            r = orc.step(U, t=t, **kw)
+            return (U, 0, t) if r is None else (r[0], 1, r[1])
+    t, steps = 0.0, 0
+    t0 = time.perf_counter()
+    while steps < max_steps and time.perf_counter() - t0 < seconds:
+        U, k, t = one(U, t)
+        steps += k
+    dt = time.perf_counter() - t0
+    return CPU_SAMPLE_N * CPU_SAMPLE_N * steps / dt, threads, kind, steps, dt
+
+
+def product_arm(args, rank, world, local_rank):
+    dist = dist_setup(world, local_rank)
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    n = args.n
+    U0 = pkg.scenarios.seeded_four_quadrant(n, n, rank)
+    prec = pkg.FP64
+    h = pkg.Handle(n, n)
+    h.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
+                CFG["strategy"], prec)
+    h.set_state(U0)
+    h.advance(args.warmup)
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    h.advance(8)  # untimed pre-roll while the clock sampler starts
+    barrier(dist)
+    done = h.advance(args.steps)
+    dev_ms, launches = h.run_stats()
+    clocks = sampler.stop()
+    barrier(dist)
+    assert done == args.steps, f"only {done} of {args.steps} steps ran"
+    dev_ms_max = allreduce_max(dist, dev_ms)
+    value = n * n * args.steps * world / (dev_ms_max / 1e3)
+    if args.kernels_only:
+        h.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "kernels_only": True,
+                "config": {"workload": f"four_quadrant_{n}x{n}_fp64"}, "clocks": clocks,
+                "gpu_launches": launches} if rank == 0 else None
+
+    # per-kernel CUDA-event durations (steps run one at a time, outside the graph);
+    # the dominant kernel is the one with the largest share of a step
+    kernel_ms, kp = h.profile_kernels(5)
+    groups = {"sweep_x": [0], "sweep_y": [1, 2], "sweep_x_final": [3], "ghost_fill": [4]}
+    alg_bytes = {"sweep_x": 64 * n * n, "sweep_y": 64 * n * n, "sweep_x_final": 96 * n * n,
+                 "ghost_fill": 64 * (4 * n + 4 * (n - 4))}
+    step_ms = sum(kernel_ms)
+    share = {g: sum(kernel_ms[q] for q in ix) / step_ms for g, ix in groups.items()}
+    top = max(share, key=share.get)
+    top_ms = sum(kernel_ms[q] for q in groups[top]) / len(groups[top])
+    peak, peak_kind = peak_hbm()
+    achieved = alg_bytes[top] / (top_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    if os.path.exists(tp) and n == N_CELLS:
+        with open(tp) as f:
+            traffic = json.load(f).get(top)
+
+    # L1 difference of the FMA product from the contraction-free build on the same steps
+    hs = pkg.Handle(n, n)
+    hs.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
+                 CFG["strategy"], pkg.FP64_STRICT)
+    hs.set_state(U0)
+    hs.advance(args.warmup + 8 + args.steps + kp)
+    A, B = h.get_state(4), hs.get_state(4)
+    l1 = [float(np.abs(A[..., f] - B[..., f]).sum() / np.abs(B[..., f]).sum()) for f in range(4)]
+    hs.close()
+
+    # e2e through the C ABI with pinned host buffers
+    import torch
+    pin_in = torch.empty((n, n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    pin_out = torch.empty((n, n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    pin_in[:] = U0
+    for _ in range(2):  # warm the e2e path
+        h.set_state_ptr(pin_in.ctypes.data, 4)
+        h.advance(1)
+        h.get_state_ptr(pin_out.ctypes.data, 4)
+    barrier(dist)
+    t0 = time.perf_counter()
+    h.set_state_ptr(pin_in.ctypes.data, 4)
+    e2e_launches = 0
+    for _ in range(args.steps):
+        h.advance(1)
+        _t, _s, _dt = h.time()
+        e2e_launches += h.run_stats()[1]
+    h.get_state_ptr(pin_out.ctypes.data, 4)
+    e2e_s = allreduce_max(dist, time.perf_counter() - t0)
+    e2e = n * n * args.steps * world / e2e_s
+    state_bytes = n * n * 4 * 8
+    h.close()
+
+    out = None
+    if rank == 0:
+        cpu_v, cores, kind, csteps, cs = cpu_reference_rate(pkg)
+        ref_cuda = None
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import REF_GPU, run_ref_gpu
+        if os.path.exists(REF_GPU):
+            rsteps = min(args.steps, 20)
+            _, rs, _, loop_ms, kms = run_ref_gpu(U0, max_steps=rsteps, **{k: CFG[k] for k in
+                                                 ("width", "height", "cfl", "alpha", "gamma", "t_end", "strategy")})
+            ref_cuda = {"value": n * n * rs / (loop_ms / 1e3), "unit": UNIT, "steps": rs,
+                        "ms_per_step": loop_ms / rs, "timer": "its own loop timer (wrappers.cuh:193,286-288)",
+                        "speedup_of_value": value / world / (n * n * rs / (loop_ms / 1e3))}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"four_quadrant_{n}x{n}_fp64", "nx": n, "ny": n, "ghost": "outflow",
+                       "cfl": CFG["cfl"], "alpha": CFG["alpha"], "gamma": CFG["gamma"], "seed": "rank",
+                       "arithmetic": "FP64, FMA contraction (nvcc default)",
+                       "l2": "inputs larger than L2 (three 537 MB state buffers)",
+                       "parallelism": f"replicas x{world}"},
+            "l1_rel_vs_reference_order": {"fields": ["rho", "p", "u", "v"], "value": l1,
+                                          "against": "contraction-free build, bit-exact with the reference -fmad=false",
+                                          "steps": args.warmup + 8 + args.steps + kp},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": 64 + state_bytes / args.steps,
+                    "path": "fvm2d_set_state(pinned) + steps x fvm2d_advance(1) + fvm2d_get_state(pinned)"},
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes[top], "ms_per_launch": top_ms,
+                         "share_of_step": share,
+                         "kernel_ms": dict(zip(["sweep_x", "sweep_y_1", "sweep_y_2", "sweep_x_final", "ghost_fill"],
+                                               kernel_ms))},
+            "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} four-quadrant, {csteps} steps in {cs:.1f} s"},
+            "reference_cuda": ref_cuda,
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "e2e_gpu_launches": e2e_launches,
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, RefHost
+    threads = os.cpu_count() or 1
+    kw = dict(CFG)
+    U = pkg.scenarios.seeded_four_quadrant(CPU_SAMPLE_N, CPU_SAMPLE_N, 0)
+    if RefHost.available():
+        ref, kind = RefHost(threads=threads), "reference"
+
+        def one(U, t):
+            V, k, tt = ref.run(U, t0=t, max_steps=1, **kw)
+            return V, tt
+    else:
+        orc, kind = Oracle(threads=threads), "port"
+
+        def one(U, t):
+            V, tt, _ = orc.step(U, t=t, **kw)
+            return V, tt
+    t = 0.0
+    for _ in range(args.warmup):
+        U, t = one(U, t)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        U, t = one(U, t)
+    secs = time.perf_counter() - t0
+    v = CPU_SAMPLE_N * CPU_SAMPLE_N * args.steps / secs
+    sample = f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} sample of the four-quadrant workload, one time step per step"
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"four_quadrant_{N_CELLS}x{N_CELLS}_fp64", "nx": N_CELLS, "ny": N_CELLS,
+                   "ghost": "outflow", "cfl": CFG["cfl"], "alpha": CFG["alpha"], "gamma": CFG["gamma"],
+                   "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N}"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["product", "reference"], default="product")
+    ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side incl. ghosts (profiling cases)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the device-resident steps only (profiling cases; no e2e or baselines)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    rank, world, local_rank = rank_info()
+    if args.impl == "reference":
+        out = reference_arm(args, rank, world)
+    else:
+        out = product_arm(args, rank, world, local_rank)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

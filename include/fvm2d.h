@@ -142,6 +142,20 @@ int fvm2d_get_time_stages_count(fvm2d_solver *s, long long *count);
  * reference keeps them in solve()'s locals, src/wrappers.cuh:191-196). */
 int fvm2d_get_time(fvm2d_solver *s, double *t, int *steps, double *last_dt);
 
+/* CUDA-event time (on the handle's stream) of the last solve()/advance()
+ * loop, and the number of kernels it launched (graph replays launch every
+ * captured kernel; steps after the loop ends exit at once).  No reference
+ * counterpart: the reference times its loop on the host only
+ * (src/wrappers.cuh:193,286-288). */
+int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_launches);
+
+/* Runs up to nsteps steps one at a time outside the graph, with CUDA events
+ * between the five kernels of a step (sweep X, sweep Y, sweep Y, final sweep X
+ * + average, ghost ring); kernel_ms[0..4] receive their mean durations in
+ * milliseconds and *steps_done the steps taken.  Advances the state like
+ * fvm2d_advance.  No reference counterpart (diagnostics). */
+int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
+
 #ifdef __cplusplus
 }
 #endif
