@@ -44,6 +44,10 @@ SIGNATURES = [
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
     ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_advance_noalloc", ctypes.c_int,
+     [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _dp,
+      ctypes.POINTER(ctypes.c_int)]),
 ]
 
 _LIB = None

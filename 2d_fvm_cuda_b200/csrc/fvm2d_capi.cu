@@ -95,6 +95,8 @@ bool is_device_pointer(const void *p)
 
 } // namespace
 
+int fvm2d::report_error(int code, const char *msg) { return fail(code, msg); }
+
 struct fvm2d_solver {
     int device = 0;
     int nx = 0, ny = 0, pitch = 0;

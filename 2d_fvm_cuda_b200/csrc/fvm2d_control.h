@@ -56,4 +56,7 @@ constexpr int kStepKernels = 5;
 FVM2D_DECLARE_VARIANT(fp64)
 FVM2D_DECLARE_VARIANT(fp64_strict)
 
+// Records `msg` as the calling thread's fvm2d_last_error() text; returns code.
+int report_error(int code, const char *msg);
+
 } // namespace fvm2d

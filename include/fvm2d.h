@@ -156,6 +156,39 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
  * fvm2d_advance.  No reference counterpart (diagnostics). */
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
 
+/* Largest nx * ny that fvm2d_advance_noalloc accepts. */
+#define FVM2D_NOALLOC_MAX_CELLS 262144
+
+/* Advances a state that lives in the caller's device memory by up to nsteps
+ * FP64 split steps from time t0, without allocating any device memory.  No
+ * counterpart in the reference (whose solve() allocates all its buffers).
+ *
+ * For callers that must not call cudaMalloc/cudaFree: applications whose
+ * device memory belongs to their own allocator or fixed-budget arena, and
+ * latency-critical loops that cannot pay for an allocation that may
+ * synchronize the device.  The intermediate buffers of the sweeps and the
+ * step-control record live in one static device array of the library, sized
+ * for FVM2D_NOALLOC_MAX_CELLS cells (16 MiB + 256 B per GPU that loads the
+ * library, held until exit); larger states are rejected with
+ * FVM2D_ERR_INVALID.
+ *
+ * state_in, state_out: device memory, 4 planes (rho, p, u, v) of ny x nx
+ *   doubles each, row-major, planes back to back; they may be the same
+ *   buffer.  The result (and the whole ring of ghost cells) lands in
+ *   state_out.
+ * Parameters as the solver setters (fvm2d_set_spatial_layout, ...), t_end
+ *   bounding the run as the reference's end time does; *t_out and
+ *   *steps_out (may be NULL) receive the time reached and the steps taken.
+ * stream: a cudaStream_t (NULL for the default stream); the call returns
+ *   after the work on it has finished.
+ * The first call on each device finds the device address of the static
+ * array and sets kernel attributes; make that first call before any stream
+ * capture.  All calls share the array: calls whose GPU work overlaps race on
+ * it, so serialize them. */
+int fvm2d_advance_noalloc(const double *state_in, double *state_out, int nx, int ny, double width, double height,
+                          double t_end, double cfl, double alpha, double gamma, int strategy, double t0,
+                          int nsteps, void *stream, double *t_out, int *steps_out);
+
 #ifdef __cplusplus
 }
 #endif
