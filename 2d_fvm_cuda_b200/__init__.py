@@ -11,5 +11,5 @@ The package directory name starts with a digit, so import it with
   workloads).
 """
 from . import scenarios  # noqa: F401
-from ._lib import FP64, FP64_STRICT, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
+from ._lib import FP32, FP64, FP64_REFORDER, FP64_STRICT, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
 from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

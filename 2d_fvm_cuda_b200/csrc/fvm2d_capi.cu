@@ -56,31 +56,48 @@ const Variant kVariants[] = {
     {fvm2d::fp64::prepare, fvm2d::fp64::enqueue_init, fvm2d::fp64::enqueue_plan, fvm2d::fp64::enqueue_step},
     {fvm2d::fp64_strict::prepare, fvm2d::fp64_strict::enqueue_init, fvm2d::fp64_strict::enqueue_plan,
      fvm2d::fp64_strict::enqueue_step},
+    {fvm2d::fp64_reforder::prepare, fvm2d::fp64_reforder::enqueue_init, fvm2d::fp64_reforder::enqueue_plan,
+     fvm2d::fp64_reforder::enqueue_step},
+    {fvm2d::fp32::prepare, fvm2d::fp32::enqueue_init, fvm2d::fp32::enqueue_plan, fvm2d::fp32::enqueue_step},
 };
+
+// Element type of the state planes for a precision: FP32 stores floats, the
+// FP64 builds doubles.  Host-side states are always doubles.
+bool is_fp32(int precision) { return precision == FVM2D_FP32; }
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-// AoS (stride doubles per cell, row-major) <-> SoA planes with a row pitch.
-__global__ void aos_to_soa(const double *__restrict__ in, int stride, double *__restrict__ U, int nx, int ny,
-                           int pitch, long long plane)
+// AoS (stride doubles per cell, row-major) <-> SoA planes of T with a row pitch.
+template <typename T>
+__global__ void aos_to_soa(const double *__restrict__ in, int stride, T *__restrict__ U, int nx, int ny, int pitch,
+                           long long plane)
 {
     const long long n = (long long)nx * ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int y = int(k / nx), x = int(k % nx);
         const long long o = (long long)y * pitch + x;
-        for (int f = 0; f < 4; ++f) U[f * plane + o] = in[k * stride + f];
+        for (int f = 0; f < 4; ++f) U[f * plane + o] = T(in[k * stride + f]);
     }
 }
 
-__global__ void soa_to_aos(const double *__restrict__ U, int nx, int ny, int pitch, long long plane, int stride,
+template <typename T>
+__global__ void soa_to_aos(const T *__restrict__ U, int nx, int ny, int pitch, long long plane, int stride,
                            double *__restrict__ out)
 {
     const long long n = (long long)nx * ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int y = int(k / nx), x = int(k % nx);
         const long long o = (long long)y * pitch + x;
-        for (int f = 0; f < 4; ++f) out[k * stride + f] = U[f * plane + o];
+        for (int f = 0; f < 4; ++f) out[k * stride + f] = double(U[f * plane + o]);
         for (int f = 4; f < stride; ++f) out[k * stride + f] = 0.0;
     }
+}
+
+// Element-wise conversion of the 4 state planes between storage types.
+template <typename S, typename D>
+__global__ void convert_planes(const S *__restrict__ in, D *__restrict__ out, long long n)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        out[k] = D(in[k]);
 }
 
 bool is_device_pointer(const void *p)
@@ -236,7 +253,11 @@ int upload(fvm2d_solver *s, const double *cells, int stride)
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
-    aos_to_soa<<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, s->U, s->nx, s->ny, s->pitch, s->plane);
+    if (is_fp32(s->precision))
+        aos_to_soa<float><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, reinterpret_cast<float *>(s->U), s->nx,
+                                                          s->ny, s->pitch, s->plane);
+    else
+        aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, s->U, s->nx, s->ny, s->pitch, s->plane);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     s->have_state = true;
@@ -330,7 +351,27 @@ SETTER(fvm2d_set_alpha, alpha, double, v == v, "alpha must be a number")
 SETTER(fvm2d_set_gamma, gamma, double, v > 1.0, "gamma must exceed 1")
 SETTER(fvm2d_set_ghost_strategy, strategy, int, v >= FVM2D_OUTFLOW && v <= FVM2D_REFLECTIVE_TB,
        "unknown ghost-cell strategy")
-SETTER(fvm2d_set_precision, precision, int, v >= 0 && v < kNumVariants, "unknown precision")
+int fvm2d_set_precision(fvm2d_solver *s, int v)
+{
+    if (int rc = check(s)) return rc;
+    if (!(v >= 0 && v < kNumVariants)) return fail(FVM2D_ERR_INVALID, "unknown precision");
+    if (s->have_state && is_fp32(v) != is_fp32(s->precision)) {
+        // keep the current state: convert its planes to the new storage type
+        const long long n = 4 * s->plane;
+        if (is_fp32(v))
+            convert_planes<double, float><<<148 * 4, 256, 0, s->stream>>>(s->U, reinterpret_cast<float *>(s->scratch), n);
+        else
+            convert_planes<float, double><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U),
+                                                                          s->scratch, n);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(s->U, s->scratch, n * (is_fp32(v) ? sizeof(float) : sizeof(double)),
+                           cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    s->precision = v;
+    s->drop_graph();
+    return FVM2D_OK;
+}
 
 int fvm2d_set_spatial_layout(fvm2d_solver *s, double width, double height)
 {
@@ -382,7 +423,11 @@ int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride)
     if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
-    soa_to_aos<<<148 * 4, 256, 0, s->stream>>>(s->U, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    if (is_fp32(s->precision))
+        soa_to_aos<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->nx, s->ny, s->pitch,
+                                                          s->plane, stride, s->scratch);
+    else
+        soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
     CK(cudaGetLastError());
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

@@ -44,7 +44,7 @@ struct LaunchConfig {
 constexpr int kStepKernels = 5;
 
 // The entry points each build of the kernels provides (namespaces fp64,
-// fp64_strict, ...).
+// fp64_strict, fp64_reforder, fp32).
 #define FVM2D_DECLARE_VARIANT(ns)                                              \
     namespace ns {                                                             \
     cudaError_t prepare();                                                     \
@@ -55,6 +55,8 @@ constexpr int kStepKernels = 5;
 
 FVM2D_DECLARE_VARIANT(fp64)
 FVM2D_DECLARE_VARIANT(fp64_strict)
+FVM2D_DECLARE_VARIANT(fp64_reforder)
+FVM2D_DECLARE_VARIANT(fp32)
 
 // Records `msg` as the calling thread's fvm2d_last_error() text; returns code.
 int report_error(int code, const char *msg);

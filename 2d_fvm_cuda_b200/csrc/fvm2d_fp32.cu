@@ -1,0 +1,12 @@
+// fvm2d_fp32.cu -- FP32 storage and arithmetic (FVM2D_FP32): the hoisted
+// physics in single precision with the compensated conservative update; the
+// wave-speed reduction, dt and time stay in FP64.  Reports its error against
+// the FP64 path rather than matching the reference bit for bit.
+#define FVM2D_VARIANT fp32
+#define FVM2D_REAL float
+#define FVM2D_PHYS HoistedCompensated
+// resident sweep blocks per SM (128 threads each) that the register
+// budget is fitted to
+#define FVM2D_X_MINB 6
+#define FVM2D_Y_MINB 6
+#include "fvm2d_variant.inc"

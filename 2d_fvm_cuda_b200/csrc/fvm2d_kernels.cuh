@@ -5,24 +5,22 @@
 // size from a device-resident control record so the loop never waits on the
 // host:
 //
-//   sweep<X>        U -> A         first sweep of branch A
-//   sweep<Y>        U -> B         first sweep of branch B
-//   sweep<Y>        A -> U         second sweep of branch A (U^n is dead now)
-//   sweep<X,final>  B -> U         second sweep of branch B, fused with the
-//                                  primitive average against U (branch A) and
-//                                  the wave-speed max of the interior cells
-//   ghost_fill      U -> U         boundary ring for the preset, wave-speed
-//                                  max of the ring, and (last block) the time
-//                                  advance plus the next step's dt
+//   sweep_x        U -> A         first sweep of branch A
+//   sweep_y        U -> B         first sweep of branch B
+//   sweep_y        A -> U         second sweep of branch A (U^n is dead now)
+//   sweep_x final  B -> U         second sweep of branch B, fused with the
+//                                 primitive average against U (branch A) and
+//                                 the wave-speed max of the interior cells
+//   ghost_kernel   U -> U         boundary ring for the preset, wave-speed
+//                                 max of the ring, and (last block) the time
+//                                 advance plus the next step's dt
 //
-// Each sweep stages a tile of cells with a two-cell halo along the sweep
-// line in shared memory, computes every limited slope once, every interface
-// (relaxation GRP + midpoint flux) once, and every cell update once; the
-// reference's slope, face-state, interface and transposed buffers never
-// reach HBM.  The y-sweep indexes rows in reverse (line position l = ny-1-j)
-// with (un, ut) = (v, u), which is the reference's anti-transpose
-// (src/basicFuns.cuh:249-262) applied inside the tile instead of through
-// global memory.
+// Every limited slope, interface (relaxation GRP + midpoint flux) and cell
+// update lives in registers; the reference's slope, face-state, interface
+// and transposed buffers never reach HBM.  The y-sweep indexes rows in
+// reverse (line position l = ny-1-j) with (un, ut) = (v, u), which is the
+// reference's anti-transpose (src/basicFuns.cuh:249-262) applied in the
+// indexing instead of through global memory.
 #pragma once
 
 #include "fvm2d_control.h"
@@ -144,192 +142,159 @@ __global__ void __launch_bounds__(NT) init_kernel(Field<Real> U, int nx, int ny,
 }
 
 // ---------------------------------------------------------------------------
-// Sweep kernel.
+// Sweep kernels.  Neither uses shared memory or a block barrier: every warp
+// works on its own pieces of the array, so a warp waiting on FP64 latency
+// never holds others back.  Both walk the array with a grid-stride loop over
+// work items; the grid is sized to the kernel's occupancy.
 //
-// DIR 0: x-sweep; a tile is NL rows x TL interfaces along x.
-// DIR 1: y-sweep; a tile is NL columns x TL interfaces along y.
-// Tile t covers updated line positions [2 + t(TL-1), 2 + t(TL-1) + TL-1)
-// and reads positions [l0-2, l0+TL].  Shared memory is laid out so that the
-// x index is the fastest-varying one in both directions, keeping global
-// loads and stores coalesced.
+// x-sweep: a work item is 32 consecutive interfaces of one row.  Lane k owns
+// interface l-1/2 with l = 2 + 31*seg + k (between cells l-1 and l): it loads
+// cells l-2..l+1, computes the two limited slopes it needs, the interface
+// flux, and receives the flux of interface l+1/2 from lane k+1 by shuffle to
+// update cell l.  Lane 31 only supplies its flux, so items advance by 31
+// cells.
+//
+// y-sweep: a work item is 32 consecutive columns times one segment of T
+// interfaces along y.  Each lane walks its column in line order (line
+// position l = ny-1-j, so the "left" cell of an interface is the one below
+// it, as in the reference's anti-transposed copy) keeping the last two
+// cells, the last slope and the last flux in registers: one cell load, one
+// slope, one interface and one update per iteration.  Loads and stores of a
+// warp touch 32 consecutive doubles of a row.
 // ---------------------------------------------------------------------------
-template <int DIR, int TL, int NL>
-struct TileMap {
-    // (line offset p in [0, len), cross c in [0, NL)) <-> flat index
-    __device__ static __forceinline__ int idx(int p, int c, int len)
-    {
-        return DIR == 0 ? c * len + p : p * NL + c;
-    }
-    __device__ static __forceinline__ void split(int w, int len, int &p, int &c)
-    {
-        if (DIR == 0) { p = w % len; c = w / len; }
-        else { c = w % NL; p = w / NL; }
-    }
-};
-
-template <typename Real, int TL, int NL>
-struct SweepSmem {
-    static constexpr int CELLS = (TL + 3) * NL;
-    static constexpr int SLOPES = (TL + 1) * NL;
-    static constexpr int FLUXES = TL * NL;
-    static constexpr size_t BYTES = sizeof(Real) * 4 * (CELLS + SLOPES + FLUXES);
-};
-
-template <typename Real, int DIR, int TL, int NL, int NT, int MINB, bool FINAL>
-__global__ void __launch_bounds__(NT, MINB) sweep_kernel(SweepArgs<Real> a)
+template <typename Real>
+__device__ __forceinline__ SweepConsts<Real> sweep_consts(const SweepArgs<Real> &a, double dt)
 {
-    using M = TileMap<DIR, TL, NL>;
-    using S = SweepSmem<Real, TL, NL>;
+    SweepConsts<Real> K;
+    K.h = Real(a.h);
+    K.rh = Real(a.rh);
+    K.alpha = Real(a.alpha);
+    K.g = Real(a.gamma);
+    K.k = Real(dt);
+    K.lambda = Real(dt / a.h);
+    K.igm1 = Real(1.0 / (a.gamma - 1.0));
+    K.kappa = Real((a.gamma + 1.0) / 2.0);
+    return K;
+}
+
+template <typename Real>
+__device__ __forceinline__ Cell<Real> load_cell(const Field<Real> &F, int x, int y, int fn, int ft)
+{
+    Cell<Real> c;
+    c.rho = F.at(0, x, y);
+    c.p = F.at(1, x, y);
+    c.un = F.at(fn, x, y);
+    c.ut = F.at(ft, x, y);
+    return c;
+}
+
+template <typename Real>
+__device__ __forceinline__ void store_cell(const Field<Real> &F, int x, int y, int fn, int ft, const Cell<Real> &c)
+{
+    F.at(0, x, y) = c.rho;
+    F.at(1, x, y) = c.p;
+    F.at(fn, x, y) = c.un;
+    F.at(ft, x, y) = c.ut;
+}
+
+template <typename Real>
+__device__ __forceinline__ Cell<Real> shfl_down(const Cell<Real> &c)
+{
+    Cell<Real> o;
+    o.rho = __shfl_down_sync(0xffffffffu, c.rho, 1);
+    o.p = __shfl_down_sync(0xffffffffu, c.p, 1);
+    o.un = __shfl_down_sync(0xffffffffu, c.un, 1);
+    o.ut = __shfl_down_sync(0xffffffffu, c.ut, 1);
+    return o;
+}
+
+// Cells updated per x-sweep work item.
+constexpr int kXCells = 31;
+
+template <typename Real, class Phys, bool FINAL, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
+{
     if (!a.ctl->active) return;
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real *s_cell = reinterpret_cast<Real *>(smem_raw);  // [4][CELLS]
-    Real *s_slope = s_cell + 4 * S::CELLS;              // [4][SLOPES]
-    Real *s_flux = s_slope + 4 * S::SLOPES;             // [4][FLUXES]
-
-    const int L = DIR == 0 ? a.nx : a.ny;
-    const int NC = DIR == 0 ? a.ny : a.nx;
-    const int tile = DIR == 0 ? blockIdx.x : blockIdx.y;
-    const int ntiles = DIR == 0 ? gridDim.x : gridDim.y;
-    const int l0 = 2 + tile * (TL - 1);
-    const int c0 = (DIR == 0 ? blockIdx.y : blockIdx.x) * NL;
-    const int fn = DIR == 0 ? 2 : 3;  // plane of the normal velocity
-    const int ft = DIR == 0 ? 3 : 2;  // plane of the tangential velocity
-
-    const double dt = a.ctl->dt;
-    const Real h = Real(a.h), rh = Real(a.rh), alpha = Real(a.alpha), g = Real(a.gamma);
-    const Real k = Real(dt);
-    const Real lambda = Real(dt / a.h);
-
-    auto gx = [&](int l, int c) { return DIR == 0 ? l : c0 + c; };
-    auto gy = [&](int l, int c) { return DIR == 0 ? c0 + c : a.ny - 1 - l; };
-
-    // 1. stage cells [l0-2, l0+TL] of NL lines
-    for (int w = threadIdx.x; w < S::CELLS; w += NT) {
-        int p, c;
-        M::split(w, TL + 3, p, c);
-        const int l = l0 - 2 + p;
-        const int s = M::idx(p, c, TL + 3);
-        if (l < L && c0 + c < NC) {
-            const int x = gx(l, c), y = gy(l, c);
-            s_cell[0 * S::CELLS + s] = a.src.at(0, x, y);
-            s_cell[1 * S::CELLS + s] = a.src.at(1, x, y);
-            s_cell[2 * S::CELLS + s] = a.src.at(fn, x, y);
-            s_cell[3 * S::CELLS + s] = a.src.at(ft, x, y);
-        } else {
-            s_cell[0 * S::CELLS + s] = Real(1);
-            s_cell[1 * S::CELLS + s] = Real(1);
-            s_cell[2 * S::CELLS + s] = Real(0);
-            s_cell[3 * S::CELLS + s] = Real(0);
-        }
-    }
-    __syncthreads();
-
-    // 2. limited slopes of cells l0-1+q, q in [0, TL]  (src/basicFuns.cuh:37-68)
-    for (int w = threadIdx.x; w < S::SLOPES; w += NT) {
-        int q, c;
-        M::split(w, TL + 1, q, c);
-        const int sm = M::idx(q, c, TL + 3), s0 = M::idx(q + 1, c, TL + 3), sp = M::idx(q + 2, c, TL + 3);
-        const int d = M::idx(q, c, TL + 1);
-#pragma unroll
-        for (int f = 0; f < 4; ++f)
-            s_slope[f * S::SLOPES + d] = limited_slope(s_cell[f * S::CELLS + sm], s_cell[f * S::CELLS + s0],
-                                                       s_cell[f * S::CELLS + sp], rh, alpha);
-    }
-    __syncthreads();
-
-    // 3. one relaxation GRP + midpoint flux per interface l-1/2, l = l0+i
-    //    (src/basicFuns.cuh:75-192, 14-34)
-    for (int w = threadIdx.x; w < S::FLUXES; w += NT) {
-        int i, c;
-        M::split(w, TL, i, c);
-        const int l = l0 + i;
-        const int d = M::idx(i, c, TL);
-        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
-        if (l <= L - 2 && c0 + c < NC) {
-            const int sl = M::idx(i + 1, c, TL + 3), sr = M::idx(i + 2, c, TL + 3);
-            const int ql = M::idx(i, c, TL + 1), qr = M::idx(i + 1, c, TL + 1);
-            Cell<Real> sL, sR, fL, fR;
-            sL.rho = s_slope[0 * S::SLOPES + ql]; sL.p = s_slope[1 * S::SLOPES + ql];
-            sL.un = s_slope[2 * S::SLOPES + ql]; sL.ut = s_slope[3 * S::SLOPES + ql];
-            sR.rho = s_slope[0 * S::SLOPES + qr]; sR.p = s_slope[1 * S::SLOPES + qr];
-            sR.un = s_slope[2 * S::SLOPES + qr]; sR.ut = s_slope[3 * S::SLOPES + qr];
-            // face states U -/+ s h / 2 (src/basicFuns.cuh:69-70)
-            fL.rho = s_cell[0 * S::CELLS + sl] + sL.rho * h * Real(0.5);
-            fL.p = s_cell[1 * S::CELLS + sl] + sL.p * h * Real(0.5);
-            fL.un = s_cell[2 * S::CELLS + sl] + sL.un * h * Real(0.5);
-            fL.ut = s_cell[3 * S::CELLS + sl] + sL.ut * h * Real(0.5);
-            fR.rho = s_cell[0 * S::CELLS + sr] - sR.rho * h * Real(0.5);
-            fR.p = s_cell[1 * S::CELLS + sr] - sR.p * h * Real(0.5);
-            fR.un = s_cell[2 * S::CELLS + sr] - sR.un * h * Real(0.5);
-            fR.ut = s_cell[3 * S::CELLS + sr] - sR.ut * h * Real(0.5);
-            const Interface<Real> W = relaxation_grp(fL, fR, sL, sR, g);
-            F = midpoint_flux(W, k);
-        }
-        s_flux[0 * S::FLUXES + d] = F.rho;
-        s_flux[1 * S::FLUXES + d] = F.p;
-        s_flux[2 * S::FLUXES + d] = F.un;
-        s_flux[3 * S::FLUXES + d] = F.ut;
-    }
-    __syncthreads();
-
-    // 4. conservative update of cells l0+i, i in [0, TL-1)  (src/basicFuns.cuh:229-246);
-    //    ghost line positions 0,1 and L-2,L-1 pass through unchanged.
+    const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
+    const int nx = a.nx, ny = a.ny;
+    const int lane = threadIdx.x & 31;
+    const int nseg = (nx - 4 + kXCells - 1) / kXCells;
+    const long long nwork = (long long)nseg * ny;
+    const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
-    auto emit = [&](int l, int c, const Cell<Real> &U) {
-        const int x = gx(l, c), y = gy(l, c);
-        if (FINAL) {
-            // primitive average with branch A (src/basicFuns.cuh:264-274)
-            const Real r = (a.comb.at(0, x, y) + U.rho) * Real(0.5);
-            const Real p = (a.comb.at(1, x, y) + U.p) * Real(0.5);
-            const Real u = (a.comb.at(fn, x, y) + U.un) * Real(0.5);
-            const Real v = (a.comb.at(ft, x, y) + U.ut) * Real(0.5);
-            a.dst.at(0, x, y) = r;
-            a.dst.at(1, x, y) = p;
-            a.dst.at(fn, x, y) = u;
-            a.dst.at(ft, x, y) = v;
-            if (x >= 2 && x <= a.nx - 3 && y >= 2 && y <= a.ny - 3)
-                vmax = fmax(vmax, DIR == 0 ? wave_speed(r, p, u, v, a.gamma) : wave_speed(r, p, v, u, a.gamma));
-        } else {
-            a.dst.at(0, x, y) = U.rho;
-            a.dst.at(1, x, y) = U.p;
-            a.dst.at(fn, x, y) = U.un;
-            a.dst.at(ft, x, y) = U.ut;
+    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
+        const int y = int(w / nseg), seg = int(w % nseg);
+        const int l = 2 + seg * kXCells + lane;
+        auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
+        const Cell<Real> cm2 = ld(l - 2), cm1 = ld(l - 1), c0 = ld(l), cp1 = ld(l + 1);
+        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
+        if (l <= nx - 2) {
+            const Cell<Real> sm1 = cell_slope(cm2, cm1, c0, K);
+            const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
+            F = Phys::interface_flux(cm1, c0, sm1, s0, K);
         }
-    };
-    for (int w = threadIdx.x; w < (TL - 1) * NL; w += NT) {
-        int i, c;
-        M::split(w, TL - 1, i, c);
-        const int l = l0 + i;
-        if (l > L - 3 || c0 + c >= NC) continue;
-        const int s = M::idx(i + 2, c, TL + 3);
-        Cell<Real> U;
-        U.rho = s_cell[0 * S::CELLS + s]; U.p = s_cell[1 * S::CELLS + s];
-        U.un = s_cell[2 * S::CELLS + s]; U.ut = s_cell[3 * S::CELLS + s];
-        const int dl = M::idx(i, c, TL), dr = M::idx(i + 1, c, TL);
-        Cell<Real> FL, FR;
-        FL.rho = s_flux[0 * S::FLUXES + dl]; FL.p = s_flux[1 * S::FLUXES + dl];
-        FL.un = s_flux[2 * S::FLUXES + dl]; FL.ut = s_flux[3 * S::FLUXES + dl];
-        FR.rho = s_flux[0 * S::FLUXES + dr]; FR.p = s_flux[1 * S::FLUXES + dr];
-        FR.un = s_flux[2 * S::FLUXES + dr]; FR.ut = s_flux[3 * S::FLUXES + dr];
-        emit(l, c, conservative_update(U, FL, FR, lambda, g));
-    }
-    // pass-through lines (only the first and last tile hold them)
-    if (tile == 0 || tile == ntiles - 1) {
-        for (int w = threadIdx.x; w < 4 * NL; w += NT) {
-            const int which = w / NL, c = w % NL;
-            const int l = which < 2 ? which : L - 4 + which;  // 0, 1, L-2, L-1
-            const int p = l - (l0 - 2);
-            const bool mine = which < 2 ? (tile == 0) : (tile == ntiles - 1);
-            if (!mine || p < 0 || p > TL + 2 || c0 + c >= NC) continue;
-            const int s = M::idx(p, c, TL + 3);
-            Cell<Real> U;
-            U.rho = s_cell[0 * S::CELLS + s]; U.p = s_cell[1 * S::CELLS + s];
-            U.un = s_cell[2 * S::CELLS + s]; U.ut = s_cell[3 * S::CELLS + s];
-            emit(l, c, U);
-        }
+        const Cell<Real> FR = shfl_down(F);
+        auto emit = [&](int x, const Cell<Real> &U) {
+            if (FINAL) {
+                const Cell<Real> A = load_cell(a.comb, x, y, 2, 3);
+                Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
+                o.rho = (A.rho + U.rho) * Real(0.5);
+                o.p = (A.p + U.p) * Real(0.5);
+                o.un = (A.un + U.un) * Real(0.5);
+                o.ut = (A.ut + U.ut) * Real(0.5);
+                store_cell(a.dst, x, y, 2, 3, o);
+                if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3)
+                    vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
+            } else {
+                store_cell(a.dst, x, y, 2, 3, U);
+            }
+        };
+        if (lane < kXCells && l <= nx - 3) emit(l, Phys::update(c0, F, FR, K));
+        // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
+        if (lane < 2 && seg == 0) emit(lane, ld(lane));
+        if (lane < 2 && seg == nseg - 1) emit(nx - 2 + lane, ld(nx - 2 + lane));
     }
     if (FINAL) block_max_to<NT>(vmax, &a.ctl->smax_bits);
+}
+
+template <typename Real, class Phys, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, int T)
+{
+    if (!a.ctl->active) return;
+    const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
+    const int nx = a.nx, ny = a.ny;
+    const int lane = threadIdx.x & 31;
+    const int ncw = (nx + 31) / 32;
+    const int nseg = (ny - 4 + T - 2) / (T - 1);
+    const long long nwork = (long long)ncw * nseg;
+    const long long wstride = (long long)gridDim.x * (NT / 32);
+    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
+        const int seg = int(w / ncw), cw = int(w % ncw);
+        const int x = cw * 32 + lane;
+        const bool col = x < nx;
+        const int xc = col ? x : nx - 1;
+        const int l0 = 2 + seg * (T - 1);
+        const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
+        auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
+        Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0);
+        Cell<Real> sm1 = cell_slope(ld(l0 - 2), cm1, c0, K);
+        Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
+        for (int l = l0; l <= lend; ++l) {
+            const Cell<Real> cp1 = ld(l + 1);
+            const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
+            const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
+            Fp = F;
+            cm1 = c0;
+            c0 = cp1;
+            sm1 = s0;
+        }
+        // ghost rows pass through (y-sweeps do not update them)
+        if (col && seg == 0)
+            for (int l = 0; l < 2; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+        if (col && seg == nseg - 1)
+            for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -121,3 +121,131 @@ def sedov_1d(n: int) -> np.ndarray:
     U[:, n // 2] = (1.0, 0.4 * E0 / dx, 0.0, 0.0)
     U[:, n // 2 - 1] = (1.0, 0.4 * E0 / dx, 0.0, 0.0)
     return U
+
+
+# ---------------------------------------------------------------------------
+# Smooth and shock-interface workloads (no reference counterpart: they use the
+# periodic and reflective-wall presets this solver adds).
+# ---------------------------------------------------------------------------
+_GL3 = (np.array([-np.sqrt(0.6), 0.0, np.sqrt(0.6)]) / 2.0, np.array([5.0, 8.0, 5.0]) / 18.0)
+
+
+def _prim_from_cons(rho, mx, my, E, gamma):
+    u, v = mx / rho, my / rho
+    return np.stack([rho, (gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v)), u, v], axis=-1)
+
+
+def vortex_point(x, y, t=0.0, L=10.0, eps=5.0, xc=5.0, yc=5.0, gamma=1.4, u0=1.0, v0=1.0):
+    """Isentropic vortex (Shu) translated with the background (rho, u, v, p) =
+    (1, u0, v0, 1) on the periodic square [0, L]^2.  Returns conserved
+    (rho, rho u, rho v, E) at the points (x, y)."""
+    dx = np.mod(x - xc - u0 * t + L / 2, L) - L / 2
+    dy = np.mod(y - yc - v0 * t + L / 2, L) - L / 2
+    r2 = dx * dx + dy * dy
+    f = np.exp(0.5 * (1.0 - r2))
+    u = u0 - eps / (2 * np.pi) * f * dy
+    v = v0 + eps / (2 * np.pi) * f * dx
+    T = 1.0 - (gamma - 1.0) * eps * eps / (8 * gamma * np.pi ** 2) * f * f
+    rho = T ** (1.0 / (gamma - 1.0))
+    p = rho * T
+    return rho, rho * u, rho * v, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)
+
+
+def periodic_square_layout(n: int, L: float = 10.0):
+    """(width, height, h) for an n x n array whose interior n-4 cells span
+    exactly [0, L]: the two ghost layers on each side lie outside."""
+    h = L / (n - 4)
+    return n * h, n * h, h
+
+
+def density_modes(count: int, amplitude: float, seed: int, L: float = 10.0, kmax: int = 4):
+    """`count` seeded periodic Fourier modes a sin(2 pi kx x / L + p) sin(2 pi ky y / L + q)
+    with |a| <= amplitude and 1 <= kx, ky <= kmax; returns a function of (x, y)."""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(1, kmax + 1, size=(count, 2))
+    a = rng.uniform(-amplitude, amplitude, size=count)
+    ph = rng.uniform(0.0, 2 * np.pi, size=(count, 2))
+
+    def f(x, y):
+        out = np.zeros(np.broadcast(x, y).shape)
+        for m in range(count):
+            out += a[m] * np.sin(2 * np.pi * k[m, 0] * x / L + ph[m, 0]) * np.sin(2 * np.pi * k[m, 1] * y / L + ph[m, 1])
+        return out
+    return f
+
+
+def isentropic_vortex(n: int, t: float = 0.0, L: float = 10.0, eps: float = 5.0, gamma: float = 1.4,
+                      perturbation=None) -> np.ndarray:
+    """Cell averages (3x3 Gauss points, conserved variables) of the isentropic
+    vortex of strength eps centred at (L/2, L/2) on the background
+    (rho, u, v, p) = (1, 1, 1, 1), advected to time t, on an n x n array with
+    two periodic ghost layers.  `perturbation(x, y)` (optional) is added to the
+    density with u, v and p unchanged.  Cell (i, j) is centred at
+    x = (i-2+1/2) h, y = L - (j-2+1/2) h, h = L/(n-4) (row 0 on top)."""
+    _, _, h = periodic_square_layout(n, L)
+    xs = (np.arange(n) - 2 + 0.5) * h
+    ys = L - (np.arange(n) - 2 + 0.5) * h
+    q, w = _GL3
+    acc = np.zeros((4, n, n))
+    for a in range(3):
+        for b in range(3):
+            X = xs[None, :] + q[a] * h
+            Y = ys[:, None] + q[b] * h
+            rho, mx, my, E = vortex_point(X, Y, t, L, eps, L / 2, L / 2, gamma)
+            if perturbation is not None:
+                u, v = mx / rho, my / rho
+                p = (gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v))
+                rho = rho + perturbation(X, Y)
+                mx, my = rho * u, rho * v
+                E = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)
+            acc += w[a] * w[b] * np.stack([rho, mx, my, E])
+    return _prim_from_cons(acc[0], acc[1], acc[2], acc[3], gamma)
+
+
+def mach2_post_shock(gamma: float = 1.4, rho1: float = 1.0, p1: float = 1.0, mach: float = 2.0):
+    """Rankine-Hugoniot state behind a shock of Mach `mach` moving in +x into
+    gas at rest (rho1, p1): (rho2, p2, u2)."""
+    m2 = mach * mach
+    rho2 = rho1 * (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0)
+    p2 = p1 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (m2 - 1.0))
+    s = mach * np.sqrt(gamma * p1 / rho1)
+    return rho2, p2, s * (1.0 - rho1 / rho2)
+
+
+def shock_bubble(nx: int, ny: int, width: float = 2.0, height: float = 1.0, seed: int = 0, gamma: float = 1.4,
+                 shock_x: float = 0.1, centre=(0.4, 0.5), radius: float = 0.15, rho_bubble: float = 0.1,
+                 modes: int = 8, amplitude: float = 0.01, sub: int = 4) -> np.ndarray:
+    """Mach-2 planar shock at x = shock_x moving in +x towards a light
+    circular bubble (rho = rho_bubble, p = 1) in gas at rest (rho = 1, p = 1),
+    on an nx x ny array spanning [0, width] x [0, height] (ghosts included).
+    The bubble radius carries `modes` seeded Fourier modes whose amplitudes sum
+    to at most `amplitude` (relative).  Cells cut by the bubble edge get the
+    sub x sub sub-sample average of the two states (conserved variables)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(0.0, amplitude / modes, modes)
+    ph = rng.uniform(0.0, 2 * np.pi, modes)
+    rho2, p2, u2 = mach2_post_shock(gamma)
+    hx, hy = width / nx, height / ny
+    xs = (np.arange(nx) + 0.5) * hx
+    ys = height - (np.arange(ny) + 0.5) * hy
+    frac = np.zeros((ny, nx))
+    offs = (np.arange(sub) + 0.5) / sub - 0.5
+    for ox in offs:
+        for oy in offs:
+            X = xs[None, :] + ox * hx
+            Y = ys[:, None] + oy * hy
+            dx, dy = X - centre[0], Y - centre[1]
+            th = np.arctan2(dy, dx)
+            r = radius * (1.0 + sum(a[k] * np.cos((k + 1) * th + ph[k]) for k in range(modes)))
+            frac += (dx * dx + dy * dy < r * r)
+    frac /= sub * sub
+    U = np.empty((ny, nx, 4))
+    U[..., 0] = rho_bubble * frac + 1.0 * (1.0 - frac)
+    U[..., 1] = 1.0
+    U[..., 2] = 0.0
+    U[..., 3] = 0.0
+    post = xs[None, :] < shock_x
+    U[..., 0] = np.where(post, rho2, U[..., 0])
+    U[..., 1] = np.where(post, p2, U[..., 1])
+    U[..., 2] = np.where(post, u2, U[..., 2])
+    return U

@@ -26,8 +26,10 @@ class ghostCellStrategy(enum.IntEnum):
 
 
 class precision(enum.IntEnum):
-    fp64 = _lib.FP64                # FMA contraction as nvcc does by default
-    fp64_strict = _lib.FP64_STRICT  # no contraction: bit-exact with the reference built -fmad=false
+    fp64 = _lib.FP64                    # shared reciprocals + FMA: fastest, within relative L1 1e-10
+    fp64_strict = _lib.FP64_STRICT      # reference order, no contraction: bit-exact with the reference -fmad=false
+    fp64_reforder = _lib.FP64_REFORDER  # reference order with FMA contraction, as the reference's own build
+    fp32 = _lib.FP32                    # FP32 storage/arithmetic, compensated update, FP64 dt
 
 
 class RGRP_2D_CUDA:

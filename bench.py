@@ -344,7 +344,7 @@ def reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side incl. ghosts (profiling cases)")

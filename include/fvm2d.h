@@ -52,8 +52,15 @@ enum fvm2d_ghost_strategy {
 
 /* Arithmetic modes (no reference counterpart: the reference has one FP64 build). */
 enum fvm2d_precision {
-    FVM2D_FP64 = 0,        /* FP64, FMA contraction as nvcc does by default (the reference's build) */
-    FVM2D_FP64_STRICT = 1  /* FP64, no contraction: bit-exact with the reference built -fmad=false */
+    FVM2D_FP64 = 0,          /* FP64, shared reciprocals and FMA: the fast default, within the
+                                reference tolerance (relative L1 1e-10) */
+    FVM2D_FP64_STRICT = 1,   /* FP64, the reference's operation order, no contraction: bit-exact
+                                with the reference built -fmad=false */
+    FVM2D_FP64_REFORDER = 2, /* FP64, the reference's operation order with FMA contraction, as the
+                                reference's own (default) build computes */
+    FVM2D_FP32 = 3           /* FP32 state planes and arithmetic with a compensated conservative
+                                update; wave-speed max, dt and time stay FP64.  Host-side states
+                                remain doubles (converted on upload and download). */
 };
 
 typedef struct fvm2d_solver fvm2d_solver;
@@ -99,7 +106,8 @@ int fvm2d_set_gamma(fvm2d_solver *s, double gamma);
  * fvm2d_ghost_strategy value. */
 int fvm2d_set_ghost_strategy(fvm2d_solver *s, int strategy);
 
-/* Selects the arithmetic build (fvm2d_precision).  No reference counterpart. */
+/* Selects the arithmetic build (fvm2d_precision); an uploaded state is kept
+ * (converted when the storage type changes).  No reference counterpart. */
 int fvm2d_set_precision(fvm2d_solver *s, int precision);
 
 /* Uploads a state of ny x nx cells of `stride` doubles (4 or 5).  Replaces the

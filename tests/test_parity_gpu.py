@@ -3,9 +3,10 @@ reference's own builds.
 
 * FP64_STRICT (no FMA contraction) must equal the oracle bit for bit, step by
   step, on every ghost-cell preset, odd sizes included.
-* FP64 (contraction on, the product default) must stay within a relative L1
-  of 1e-10 per field of the oracle at the final time of the 400x400
-  four-quadrant workload (620 steps).
+* FP64 (shared reciprocals and FMA, the product default) and FP64_REFORDER
+  (reference order, FMA) must stay within a relative L1 of 1e-10 per field of
+  the oracle at the final time of the 400x400 four-quadrant workload (620
+  steps).
 * The reference's CUDA kernels (oracle/_ref/ref_gpu*) on the same GPU: the
   -fmad=false build equals FP64_STRICT bit for bit; the default build is
   within the same 1e-10 relative L1 of FP64.
@@ -91,13 +92,14 @@ def test_strict_equals_reference_fixture(pkg, golden, name):
     assert np.array_equal(U, z[f"{name}/U1"], equal_nan=True)
 
 
-def test_fma_within_tolerance_full_quadrant_workload(pkg, oracle, golden):
+@pytest.mark.parametrize("precision", [0, 2])  # FP64 (shared reciprocals), FP64_REFORDER
+def test_fma_within_tolerance_full_quadrant_workload(pkg, oracle, golden, precision):
     """400x400 incl. ghosts, [0,1]^2, gamma 1.4, outflow, CFL 0.45, t_end 0.2, alpha 1.9, seed 0."""
     z, manifest = golden
     m = manifest["quad_outflow_400x400_seed0"]
     kw = {k: m[k] for k in RUN_KEYS}
     U0 = pkg.scenarios.seeded_four_quadrant(m["nx"], m["ny"], m["seed"])
-    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64, **kw)
+    G, steps, t = gpu_run(pkg, U0, precision=precision, **kw)
     assert steps == m["steps"] and t == pytest.approx(m["t"], rel=0, abs=1e-15)
     O, osteps, ot = oracle.solve(U0, **kw)
     assert osteps == steps
@@ -118,21 +120,22 @@ def test_reference_cuda_nofma_equals_strict(pkg):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA build not present")
+@pytest.mark.parametrize("precision", [0, 2])
 @pytest.mark.parametrize("strategy", [0, 4])
-def test_reference_cuda_default_build_within_tolerance(pkg, golden, strategy):
+def test_reference_cuda_default_build_within_tolerance(pkg, golden, strategy, precision):
     z, manifest = golden
     m = manifest["quad_outflow_400x400_seed0"]
     kw = {k: m[k] for k in RUN_KEYS}
     kw["strategy"] = strategy
     U0 = pkg.scenarios.seeded_four_quadrant(400, 400, m["seed"])
     R, rsteps, rt, _, _ = run_ref_gpu(U0, fma=True, **kw)
-    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64, **kw)
+    G, steps, t = gpu_run(pkg, U0, precision=precision, **kw)
     assert steps == rsteps
     err = rel_l1(G, R)
     assert max(err) <= REL_L1_TOL, err
 
 
-@pytest.mark.parametrize("precision", [1, 0])
+@pytest.mark.parametrize("precision", [1, 0, 2])
 def test_full_size_step_commutes_with_anti_transpose(pkg, precision):
     """S(rot U) = rot S(U) at 4096^2: checks the reversed-direction y-sweep
     against the x-sweep on the whole headline-size array."""
