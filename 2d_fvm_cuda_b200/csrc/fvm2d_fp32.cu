@@ -7,6 +7,11 @@
 #define FVM2D_PHYS HoistedCompensated
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to
+#ifdef FVM2D_TUNE_X
+#define FVM2D_X_MINB FVM2D_TUNE_X
+#define FVM2D_Y_MINB FVM2D_TUNE_Y
+#else
 #define FVM2D_X_MINB 6
 #define FVM2D_Y_MINB 6
+#endif
 #include "fvm2d_variant.inc"

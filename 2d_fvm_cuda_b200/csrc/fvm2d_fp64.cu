@@ -6,6 +6,11 @@
 #define FVM2D_PHYS Hoisted
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to; measured best for this build at 4096^2
+#ifdef FVM2D_TUNE_X
+#define FVM2D_X_MINB FVM2D_TUNE_X
+#define FVM2D_Y_MINB FVM2D_TUNE_Y
+#else
 #define FVM2D_X_MINB 5
 #define FVM2D_Y_MINB 5
+#endif
 #include "fvm2d_variant.inc"

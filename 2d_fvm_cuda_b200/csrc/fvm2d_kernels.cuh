@@ -147,19 +147,19 @@ __global__ void __launch_bounds__(NT) init_kernel(Field<Real> U, int nx, int ny,
 // never holds others back.  Both walk the array with a grid-stride loop over
 // work items; the grid is sized to the kernel's occupancy.
 //
-// x-sweep: a work item is 32 consecutive interfaces of one row.  Lane k owns
-// interface l-1/2 with l = 2 + 31*seg + k (between cells l-1 and l): it loads
-// cells l-2..l+1, computes the two limited slopes it needs, the interface
-// flux, and receives the flux of interface l+1/2 from lane k+1 by shuffle to
-// update cell l.  Lane 31 only supplies its flux, so items advance by 31
-// cells.
+// x-sweep: a work item is 32 consecutive cells of one row.  Lane k holds cell
+// c = 1 + 30*seg + k: it loads cells c-1..c+1, computes the limited slope of
+// c, takes the slope of c-1 from lane k-1 by shuffle and computes the
+// interface c-1/2 (lanes 1..31), then takes the flux of c+1/2 from lane k+1 to
+// update cell c (lanes 1..30).  Items advance by 30 cells.
 //
 // y-sweep: a work item is 32 consecutive columns times one segment of T
 // interfaces along y.  Each lane walks its column in line order (line
 // position l = ny-1-j, so the "left" cell of an interface is the one below
-// it, as in the reference's anti-transposed copy) keeping the last two
-// cells, the last slope and the last flux in registers: one cell load, one
-// slope, one interface and one update per iteration.  Loads and stores of a
+// it, as in the reference's anti-transposed copy) keeping three cells, the
+// last slope and the last flux in registers: one cell load (issued one
+// iteration before its use), one slope, one interface and one update per
+// iteration.  Loads and stores of a
 // warp touch 32 consecutive doubles of a row.
 // ---------------------------------------------------------------------------
 template <typename Real>
@@ -208,8 +208,20 @@ __device__ __forceinline__ Cell<Real> shfl_down(const Cell<Real> &c)
     return o;
 }
 
-// Cells updated per x-sweep work item.
-constexpr int kXCells = 31;
+template <typename Real>
+__device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
+{
+    Cell<Real> o;
+    o.rho = __shfl_up_sync(0xffffffffu, c.rho, 1);
+    o.p = __shfl_up_sync(0xffffffffu, c.p, 1);
+    o.un = __shfl_up_sync(0xffffffffu, c.un, 1);
+    o.ut = __shfl_up_sync(0xffffffffu, c.ut, 1);
+    return o;
+}
+
+// Cells updated per x-sweep work item: lane k holds cell c = 1 + 30 seg + k;
+// lanes 1..31 own the interface c-1/2, lanes 1..30 update cell c.
+constexpr int kXCells = 30;
 
 template <typename Real, class Phys, bool FINAL, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
@@ -224,24 +236,24 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     double vmax = 0.0;
     for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
         const int y = int(w / nseg), seg = int(w % nseg);
-        const int l = 2 + seg * kXCells + lane;
+        const int c = 1 + seg * kXCells + lane;
+        const bool upd = lane >= 1 && lane <= kXCells && c <= nx - 3;
         auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
-        const Cell<Real> cm2 = ld(l - 2), cm1 = ld(l - 1), c0 = ld(l), cp1 = ld(l + 1);
+        const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
+        Cell<Real> A;
+        if (FINAL) A = load_cell(a.comb, min(c, nx - 1), y, 2, 3);  // branch A, loaded early
+        const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);           // slope of cell c
+        const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
         Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
-        if (l <= nx - 2) {
-            const Cell<Real> sm1 = cell_slope(cm2, cm1, c0, K);
-            const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
-            F = Phys::interface_flux(cm1, c0, sm1, s0, K);
-        }
+        if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
         const Cell<Real> FR = shfl_down(F);
-        auto emit = [&](int x, const Cell<Real> &U) {
+        auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
             if (FINAL) {
-                const Cell<Real> A = load_cell(a.comb, x, y, 2, 3);
                 Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
-                o.rho = (A.rho + U.rho) * Real(0.5);
-                o.p = (A.p + U.p) * Real(0.5);
-                o.un = (A.un + U.un) * Real(0.5);
-                o.ut = (A.ut + U.ut) * Real(0.5);
+                o.rho = (Ab.rho + U.rho) * Real(0.5);
+                o.p = (Ab.p + U.p) * Real(0.5);
+                o.un = (Ab.un + U.un) * Real(0.5);
+                o.ut = (Ab.ut + U.ut) * Real(0.5);
                 store_cell(a.dst, x, y, 2, 3, o);
                 if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3)
                     vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
@@ -249,10 +261,19 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
                 store_cell(a.dst, x, y, 2, 3, U);
             }
         };
-        if (lane < kXCells && l <= nx - 3) emit(l, Phys::update(c0, F, FR, K));
+        if (upd) emit(c, Phys::update(c0, F, FR, K), A);
         // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
-        if (lane < 2 && seg == 0) emit(lane, ld(lane));
-        if (lane < 2 && seg == nseg - 1) emit(nx - 2 + lane, ld(nx - 2 + lane));
+        if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
+            const int x = seg == 0 ? lane : nx - 2 + lane;
+            Cell<Real> Ab;
+            if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
+            emit(x, ld(x), Ab);
+            if (seg == 0 && seg == nseg - 1) {
+                const int x2 = nx - 2 + lane;
+                if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
+                emit(x2, ld(x2), Ab);
+            }
+        }
     }
     if (FINAL) block_max_to<NT>(vmax, &a.ctl->smax_bits);
 }
@@ -276,17 +297,18 @@ __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, in
         const int l0 = 2 + seg * (T - 1);
         const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
         auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
-        Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0);
+        Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
         Cell<Real> sm1 = cell_slope(ld(l0 - 2), cm1, c0, K);
         Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
         for (int l = l0; l <= lend; ++l) {
-            const Cell<Real> cp1 = ld(l + 1);
+            const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
             const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
             const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
             if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
             Fp = F;
             cm1 = c0;
             c0 = cp1;
+            cp1 = cp2;
             sm1 = s0;
         }
         // ghost rows pass through (y-sweeps do not update them)
