@@ -1,7 +1,9 @@
 // fvm2d_fp32.cu -- FP32 storage and arithmetic (FVM2D_FP32): the hoisted
 // physics in single precision with the compensated conservative update; the
 // wave-speed reduction, dt and time stay in FP64.  Reports its error against
-// the FP64 path rather than matching the reference bit for bit.
+// the FP64 path rather than matching the reference bit for bit.  Built with
+// -prec-div=false -prec-sqrt=false (FP32 division and square root within
+// 2 ulp).
 #define FVM2D_VARIANT fp32
 #define FVM2D_REAL float
 #define FVM2D_PHYS HoistedCompensated

@@ -229,6 +229,25 @@ def product_arm(args, rank, world, local_rank):
     l1 = [float(np.abs(A[..., f] - B[..., f]).sum() / np.abs(B[..., f]).sum()) for f in range(4)]
     hs.close()
 
+    # FP32 form on the same workload and steps: speed and density error vs FP64
+    hf = pkg.Handle(n, n)
+    hf.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
+                 CFG["strategy"], pkg.FP32)
+    hf.set_state(U0)
+    hf.advance(args.warmup + 8)
+    hf.advance(args.steps)
+    f32_ms, _ = hf.run_stats()
+    hf.advance(kp)
+    F32 = hf.get_state(4)
+    f32_l1 = [float(np.abs(F32[..., f] - A[..., f]).sum() / np.abs(A[..., f]).sum()) for f in range(4)]
+    hf.close()
+    f32_ms = allreduce_max(dist, f32_ms)
+    fp32 = {"value": n * n * args.steps * world / (f32_ms / 1e3), "unit": UNIT, "ms_per_step": f32_ms / args.steps,
+            "speedup_vs_fp64": dev_ms_max / f32_ms,
+            "l1_rel_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_l1,
+                               "steps": args.warmup + 8 + args.steps + kp},
+            "arithmetic": "FP32 planes and arithmetic, compensated update, FP64 wave-speed max and dt"}
+
     # e2e through the C ABI with pinned host buffers
     import torch
     pin_in = torch.empty((n, n, 4), dtype=torch.float64, pin_memory=True).numpy()
@@ -289,6 +308,7 @@ def product_arm(args, rank, world, local_rank):
             "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} four-quadrant, {csteps} steps in {cs:.1f} s"},
             "reference_cuda": ref_cuda,
+            "fp32": fp32,
             "clocks": clocks,
             "gpu_launches": launches,
             "e2e_gpu_launches": e2e_launches,
