@@ -7,9 +7,10 @@ The package directory name starts with a digit, so import it with
   solver interface (src/wrappers.cuh:17-65) over libfvm2d.so.
 * ``Handle`` -- one C-ABI solver handle (include/fvm2d.h), for callers that
   want the state to stay on the GPU between calls.
+* ``Batch`` -- many independent problems of different sizes solved together.
 * ``scenarios`` -- initial data (the reference's demo problems and seeded
   workloads).
 """
 from . import scenarios  # noqa: F401
-from ._lib import FP32, FP64, FP64_REFORDER, FP64_STRICT, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
+from ._lib import FP32, FP64, FP64_REFORDER, FP64_STRICT, Batch, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
 from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

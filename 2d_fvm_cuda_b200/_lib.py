@@ -44,6 +44,20 @@ SIGNATURES = [
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
     ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_batch_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_batch_destroy", ctypes.c_int, [_vp]),
+    ("fvm2d_batch_set_problem", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    ("fvm2d_batch_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("fvm2d_batch_set_state", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    ("fvm2d_batch_get_state", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    ("fvm2d_batch_solve", ctypes.c_int, [_vp]),
+    ("fvm2d_batch_get_time", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_batch_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong),
+                                                 ctypes.POINTER(ctypes.c_longlong)]),
+    ("fvm2d_batch_autotune", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_advance_noalloc", ctypes.c_int,
      [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
       ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _dp,
@@ -180,3 +194,71 @@ class Handle:
         c = ctypes.c_longlong(0)
         check(self.lib.fvm2d_get_time_stages_count(self.h, ctypes.byref(c)))
         return c.value
+
+
+class Batch:
+    """Owns one fvm2d_batch: many problems of different sizes solved together."""
+
+    def __init__(self, sizes):
+        """sizes: sequence of (nx, ny)."""
+        self.lib = load()
+        self.sizes = [(int(a), int(b)) for a, b in sizes]
+        n = len(self.sizes)
+        nx = (ctypes.c_int * n)(*[s[0] for s in self.sizes])
+        ny = (ctypes.c_int * n)(*[s[1] for s in self.sizes])
+        h = _vp()
+        check(self.lib.fvm2d_batch_create(ctypes.byref(h), n, nx, ny))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.fvm2d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_problem(self, p, width=1.0, height=1.0, t_end=0.0, cfl=0.5, alpha=1.9, gamma=1.4, strategy=0):
+        check(self.lib.fvm2d_batch_set_problem(self.h, p, width, height, t_end, cfl, alpha, gamma, int(strategy)))
+
+    def set_precision(self, precision: int) -> None:
+        check(self.lib.fvm2d_batch_set_precision(self.h, int(precision)))
+
+    def set_state(self, p, U) -> None:
+        A = as_cells(U)
+        if A.shape[:2] != (self.sizes[p][1], self.sizes[p][0]):
+            raise ValueError("state shape does not match the problem size")
+        check(self.lib.fvm2d_batch_set_state(self.h, p, A.ctypes.data, A.shape[2]))
+
+    def get_state(self, p, stride: int = 4) -> np.ndarray:
+        nx, ny = self.sizes[p]
+        out = np.empty((ny, nx, stride))
+        check(self.lib.fvm2d_batch_get_state(self.h, p, out.ctypes.data, stride))
+        return out
+
+    def solve(self) -> None:
+        check(self.lib.fvm2d_batch_solve(self.h))
+
+    def time(self, p):
+        t = ctypes.c_double(0)
+        k = ctypes.c_int(0)
+        check(self.lib.fvm2d_batch_get_time(self.h, p, ctypes.byref(t), ctypes.byref(k)))
+        return t.value, k.value
+
+    def run_stats(self):
+        """(device_ms, kernel_launches, cell_updates) of the last solve."""
+        ms = ctypes.c_double(0)
+        n = ctypes.c_longlong(0)
+        c = ctypes.c_longlong(0)
+        check(self.lib.fvm2d_batch_get_run_stats(self.h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(c)))
+        return ms.value, n.value, c.value
+
+    def autotune(self, trial_steps: int = 2):
+        """Picks the y-segment length and sweep grid size; returns them."""
+        T = ctypes.c_int(0)
+        g = ctypes.c_int(0)
+        check(self.lib.fvm2d_batch_autotune(self.h, int(trial_steps), ctypes.byref(T), ctypes.byref(g)))
+        return T.value, g.value

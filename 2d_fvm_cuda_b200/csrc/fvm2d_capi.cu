@@ -12,6 +12,7 @@
 //   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
 #include "../../include/fvm2d.h"
 #include "fvm2d_control.h"
+#include "fvm2d_transfer.cuh"
 
 #include <chrono>
 #include <climits>
@@ -23,6 +24,10 @@
 
 using fvm2d::LaunchConfig;
 using fvm2d::StepControl;
+using fvm2d::aos_to_soa;
+using fvm2d::convert_planes;
+using fvm2d::is_device_pointer;
+using fvm2d::soa_to_aos;
 
 namespace {
 
@@ -65,50 +70,6 @@ const Variant kVariants[] = {
 // FP64 builds doubles.  Host-side states are always doubles.
 bool is_fp32(int precision) { return precision == FVM2D_FP32; }
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
-
-// AoS (stride doubles per cell, row-major) <-> SoA planes of T with a row pitch.
-template <typename T>
-__global__ void aos_to_soa(const double *__restrict__ in, int stride, T *__restrict__ U, int nx, int ny, int pitch,
-                           long long plane)
-{
-    const long long n = (long long)nx * ny;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const int y = int(k / nx), x = int(k % nx);
-        const long long o = (long long)y * pitch + x;
-        for (int f = 0; f < 4; ++f) U[f * plane + o] = T(in[k * stride + f]);
-    }
-}
-
-template <typename T>
-__global__ void soa_to_aos(const T *__restrict__ U, int nx, int ny, int pitch, long long plane, int stride,
-                           double *__restrict__ out)
-{
-    const long long n = (long long)nx * ny;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const int y = int(k / nx), x = int(k % nx);
-        const long long o = (long long)y * pitch + x;
-        for (int f = 0; f < 4; ++f) out[k * stride + f] = double(U[f * plane + o]);
-        for (int f = 4; f < stride; ++f) out[k * stride + f] = 0.0;
-    }
-}
-
-// Element-wise conversion of the 4 state planes between storage types.
-template <typename S, typename D>
-__global__ void convert_planes(const S *__restrict__ in, D *__restrict__ out, long long n)
-{
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        out[k] = D(in[k]);
-}
-
-bool is_device_pointer(const void *p)
-{
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 
 } // namespace
 

@@ -223,59 +223,103 @@ __device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
 // lanes 1..31 own the interface c-1/2, lanes 1..30 update cell c.
 constexpr int kXCells = 30;
 
+// One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
+// wave speed of the interior cells written by a final sweep.
+template <typename Real, class Phys, bool FINAL>
+__device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int y, int seg,
+                                       int nseg, int lane, double &vmax)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int c = 1 + seg * kXCells + lane;
+    const bool upd = lane >= 1 && lane <= kXCells && c <= nx - 3;
+    auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
+    const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
+    Cell<Real> A;
+    if (FINAL) A = load_cell(a.comb, min(c, nx - 1), y, 2, 3);  // branch A, loaded early
+    const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);           // slope of cell c
+    const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
+    Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
+    if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+    const Cell<Real> FR = shfl_down(F);
+    auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
+        if (FINAL) {
+            Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
+            o.rho = (Ab.rho + U.rho) * Real(0.5);
+            o.p = (Ab.p + U.p) * Real(0.5);
+            o.un = (Ab.un + U.un) * Real(0.5);
+            o.ut = (Ab.ut + U.ut) * Real(0.5);
+            store_cell(a.dst, x, y, 2, 3, o);
+            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3)
+                vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
+        } else {
+            store_cell(a.dst, x, y, 2, 3, U);
+        }
+    };
+    if (upd) emit(c, Phys::update(c0, F, FR, K), A);
+    // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
+    if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
+        const int x = seg == 0 ? lane : nx - 2 + lane;
+        Cell<Real> Ab;
+        if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
+        emit(x, ld(x), Ab);
+        if (seg == 0 && seg == nseg - 1) {
+            const int x2 = nx - 2 + lane;
+            if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
+            emit(x2, ld(x2), Ab);
+        }
+    }
+}
+
 template <typename Real, class Phys, bool FINAL, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
 {
     if (!a.ctl->active) return;
     const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
-    const int nx = a.nx, ny = a.ny;
     const int lane = threadIdx.x & 31;
-    const int nseg = (nx - 4 + kXCells - 1) / kXCells;
-    const long long nwork = (long long)nseg * ny;
+    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
+    const long long nwork = (long long)nseg * a.ny;
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
-    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
-        const int y = int(w / nseg), seg = int(w % nseg);
-        const int c = 1 + seg * kXCells + lane;
-        const bool upd = lane >= 1 && lane <= kXCells && c <= nx - 3;
-        auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
-        const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
-        Cell<Real> A;
-        if (FINAL) A = load_cell(a.comb, min(c, nx - 1), y, 2, 3);  // branch A, loaded early
-        const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);           // slope of cell c
-        const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
-        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
-        if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
-        const Cell<Real> FR = shfl_down(F);
-        auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
-            if (FINAL) {
-                Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
-                o.rho = (Ab.rho + U.rho) * Real(0.5);
-                o.p = (Ab.p + U.p) * Real(0.5);
-                o.un = (Ab.un + U.un) * Real(0.5);
-                o.ut = (Ab.ut + U.ut) * Real(0.5);
-                store_cell(a.dst, x, y, 2, 3, o);
-                if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3)
-                    vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
-            } else {
-                store_cell(a.dst, x, y, 2, 3, U);
-            }
-        };
-        if (upd) emit(c, Phys::update(c0, F, FR, K), A);
-        // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
-        if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
-            const int x = seg == 0 ? lane : nx - 2 + lane;
-            Cell<Real> Ab;
-            if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
-            emit(x, ld(x), Ab);
-            if (seg == 0 && seg == nseg - 1) {
-                const int x2 = nx - 2 + lane;
-                if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
-                emit(x2, ld(x2), Ab);
-            }
-        }
-    }
+    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+        x_item<Real, Phys, FINAL>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax);
     if (FINAL) block_max_to<NT>(vmax, &a.ctl->smax_bits);
+}
+
+// Segments of T interfaces (T-1 updated cells) along a y line of ny cells.
+__host__ __device__ __forceinline__ int y_segments(int ny, int T) { return (ny - 4 + T - 2) / (T - 1); }
+
+// One y-sweep work item: columns 32 cw .. 32 cw + 31, segment seg (of nseg)
+// of T interfaces.
+template <typename Real, class Phys>
+__device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int seg, int nseg,
+                                       int cw, int lane, int T)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int x = cw * 32 + lane;
+    const bool col = x < nx;
+    const int xc = col ? x : nx - 1;
+    const int l0 = 2 + seg * (T - 1);
+    const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
+    auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
+    Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
+    Cell<Real> sm1 = cell_slope(ld(l0 - 2), cm1, c0, K);
+    Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
+    for (int l = l0; l <= lend; ++l) {
+        const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
+        const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
+        const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+        if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
+        Fp = F;
+        cm1 = c0;
+        c0 = cp1;
+        cp1 = cp2;
+        sm1 = s0;
+    }
+    // ghost rows pass through (y-sweeps do not update them)
+    if (col && seg == 0)
+        for (int l = 0; l < 2; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+    if (col && seg == nseg - 1)
+        for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
 }
 
 template <typename Real, class Phys, int NT, int MINB>
@@ -283,40 +327,13 @@ __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, in
 {
     if (!a.ctl->active) return;
     const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
-    const int nx = a.nx, ny = a.ny;
     const int lane = threadIdx.x & 31;
-    const int ncw = (nx + 31) / 32;
-    const int nseg = (ny - 4 + T - 2) / (T - 1);
+    const int ncw = (a.nx + 31) / 32;
+    const int nseg = y_segments(a.ny, T);
     const long long nwork = (long long)ncw * nseg;
     const long long wstride = (long long)gridDim.x * (NT / 32);
-    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
-        const int seg = int(w / ncw), cw = int(w % ncw);
-        const int x = cw * 32 + lane;
-        const bool col = x < nx;
-        const int xc = col ? x : nx - 1;
-        const int l0 = 2 + seg * (T - 1);
-        const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
-        auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
-        Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
-        Cell<Real> sm1 = cell_slope(ld(l0 - 2), cm1, c0, K);
-        Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
-        for (int l = l0; l <= lend; ++l) {
-            const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
-            const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
-            const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
-            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
-            Fp = F;
-            cm1 = c0;
-            c0 = cp1;
-            cp1 = cp2;
-            sm1 = s0;
-        }
-        // ghost rows pass through (y-sweeps do not update them)
-        if (col && seg == 0)
-            for (int l = 0; l < 2; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
-        if (col && seg == nseg - 1)
-            for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
-    }
+    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+        y_item<Real, Phys>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T);
 }
 
 // ---------------------------------------------------------------------------
@@ -438,47 +455,59 @@ __device__ __forceinline__ Cell<Real> col_rule(const GhostArgs<Real> &a, int i, 
     }
 }
 
-// One thread per ring cell: 4 rows x nx, then 4 columns x (ny - 4).
+// Ring cell k of 4 nx + 4 (ny - 4): rows 0, 1, ny-2, ny-1 first, then
+// columns 0, 1, nx-2, nx-1 of rows 2..ny-3.  Writes the cell and returns its
+// wave speed.
+template <typename Real>
+__device__ __forceinline__ double ghost_cell(const GhostArgs<Real> &a, int k, double t)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int nrow = 4 * nx;
+    int i, j;
+    if (k < nrow) {
+        const int r = k / nx;
+        i = k % nx;
+        j = r < 2 ? r : ny - 4 + r;
+    } else {
+        const int q = k - nrow;
+        const int r = q / (ny - 4);
+        j = 2 + q % (ny - 4);
+        i = r < 2 ? r : nx - 4 + r;
+    }
+    const bool gcol = i < 2 || i >= nx - 2;
+    const Cell<Real> c = gcol ? col_rule(a, i, j, t) : row_rule(a, i, j, t);
+    a.U.at(0, i, j) = c.rho;
+    a.U.at(1, i, j) = c.p;
+    a.U.at(2, i, j) = c.un;
+    a.U.at(3, i, j) = c.ut;
+    return wave_speed(c.rho, c.p, c.un, c.ut, a.gamma);
+}
+
+// Commits the step in flight (t += dt, steps + 1), takes the running wave-speed
+// max as the new state's, and plans the next step.  One thread, after every
+// contribution to smax_bits is visible.
+__device__ __forceinline__ void finish_step(StepControl *ctl, const PlanParams &plan)
+{
+    volatile StepControl *vc = ctl;
+    ctl->t = vc->t + vc->dt;
+    ctl->steps = vc->steps + 1;
+    ctl->smax_last = __longlong_as_double((long long)vc->smax_bits);
+    ctl->smax_bits = 0ull;
+    ctl->ticket = 0u;
+    plan_step(ctl, plan);
+}
+
+// One thread per ring cell.
 template <typename Real, int NT>
 __global__ void __launch_bounds__(NT) ghost_kernel(GhostArgs<Real> a)
 {
     StepControl *ctl = a.ctl;
     if (!ctl->active) return;
     const double t = ctl->t + ctl->dt;  // the fill sees the advanced time (wrappers.cuh:250,265-280)
-    const int nx = a.nx, ny = a.ny;
-    const int nrow = 4 * nx, ncol = 4 * (ny - 4);
     const int k = blockIdx.x * NT + threadIdx.x;
-    double vmax = 0.0;
-    if (k < nrow + ncol) {
-        int i, j;
-        if (k < nrow) {
-            const int r = k / nx;
-            i = k % nx;
-            j = r < 2 ? r : ny - 4 + r;
-        } else {
-            const int q = k - nrow;
-            const int r = q / (ny - 4);
-            j = 2 + q % (ny - 4);
-            i = r < 2 ? r : nx - 4 + r;
-        }
-        const bool gcol = i < 2 || i >= nx - 2;
-        const Cell<Real> c = gcol ? col_rule(a, i, j, t) : row_rule(a, i, j, t);
-        a.U.at(0, i, j) = c.rho;
-        a.U.at(1, i, j) = c.p;
-        a.U.at(2, i, j) = c.un;
-        a.U.at(3, i, j) = c.ut;
-        vmax = wave_speed(c.rho, c.p, c.un, c.ut, a.gamma);
-    }
+    const double vmax = (k < 4 * a.nx + 4 * (a.ny - 4)) ? ghost_cell(a, k, t) : 0.0;
     block_max_to<NT>(vmax, &ctl->smax_bits);
-    if (last_block_done(&ctl->ticket)) {
-        volatile StepControl *vc = ctl;
-        ctl->t = vc->t + vc->dt;
-        ctl->steps = vc->steps + 1;
-        ctl->smax_last = __longlong_as_double((long long)vc->smax_bits);
-        ctl->smax_bits = 0ull;
-        ctl->ticket = 0u;
-        plan_step(ctl, a.plan);
-    }
+    if (last_block_done(&ctl->ticket)) finish_step(ctl, a.plan);
 }
 
 } // namespace FVM2D_VARIANT

@@ -19,11 +19,15 @@ POST_SHOCK_2MACH = (8.0, 116.5, 4.125 * math.sqrt(3.0), -4.125)
 PRE_SHOCK_2MACH = (1.4, 1.0, 0.0, 0.0)
 
 
-def four_quadrant(U1, U2, U3, U4, nx: int, ny: int) -> np.ndarray:
+def four_quadrant(U1, U2, U3, U4, nx: int, ny: int, split=None) -> np.ndarray:
     """Four constant states split at (nx/2, ny/2): U2 | U1 over U3 | U4
-    (src/wrappers.cuh:80-108, RGRP_2D_CUDA::setRPInitialData)."""
+    (src/wrappers.cuh:80-108, RGRP_2D_CUDA::setRPInitialData).  `split`
+    (fractions (sx, sy) of the width and height, measured from the left and
+    from the top row) moves the split point."""
     U = np.empty((ny, nx, 4))
     hx, hy = nx // 2, ny // 2
+    if split is not None:
+        hx, hy = int(round(split[0] * nx)), int(round(split[1] * ny))
     U[:hy, :hx] = U2[:4]
     U[hy:, :hx] = U3[:4]
     U[:hy, hx:] = U1[:4]
@@ -45,9 +49,23 @@ def seeded_quadrant_states(seed: int):
     return out
 
 
-def seeded_four_quadrant(nx: int, ny: int, seed: int) -> np.ndarray:
-    """The seeded four-quadrant Riemann problem split at the domain centre."""
-    return four_quadrant(*seeded_quadrant_states(seed), nx, ny)
+def seeded_four_quadrant(nx: int, ny: int, seed: int, split=None) -> np.ndarray:
+    """The seeded four-quadrant Riemann problem split at the domain centre (or
+    at `split`, see four_quadrant)."""
+    return four_quadrant(*seeded_quadrant_states(seed), nx, ny, split)
+
+
+def uneven_batch(count: int, seed: int, sizes=tuple(range(128, 1025, 64))):
+    """`count` seeded four-quadrant problems for the batched form: per-side
+    size drawn from `sizes`, split point ~U[0.3, 0.7]^2, states as
+    seeded_quadrant_states.  Returns a list of (nx, ny, seed, split)."""
+    r = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(r.choice(sizes))
+        split = (float(r.uniform(0.3, 0.7)), float(r.uniform(0.3, 0.7)))
+        out.append((n, n, int(r.integers(0, 2 ** 31 - 1)), split))
+    return out
 
 
 def double_mach(n: int) -> np.ndarray:

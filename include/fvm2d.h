@@ -164,6 +164,50 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
  * fvm2d_advance.  No reference counterpart (diagnostics). */
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
 
+/* ---- batched form (no reference counterpart) -------------------------------
+ * Many independent problems of different sizes advance together: every stage
+ * of the step is one launch covering all problems, each problem with its own
+ * dt, end time and ghost preset, and the time loop is captured in CUDA
+ * graphs.  Results match the same problems solved one by one with the same
+ * precision bit for bit. */
+typedef struct fvm2d_batch fvm2d_batch;
+
+/* A batch of nproblems problems; problem p is nx[p] x ny[p] cells (ghosts
+ * included, >= 6 each) on the current device.  Per-problem defaults as
+ * fvm2d_create. */
+int fvm2d_batch_create(fvm2d_batch **out, int nproblems, const int *nx, const int *ny);
+int fvm2d_batch_destroy(fvm2d_batch *b);
+
+/* The setters of the solver (setSpatialLayout, setTimeLayout, setAlpha,
+ * setGamma, setGhostCellStrategy; src/wrappers.cuh:110-145) for problem p. */
+int fvm2d_batch_set_problem(fvm2d_batch *b, int p, double width, double height, double t_end, double cfl,
+                            double alpha, double gamma, int strategy);
+
+/* Arithmetic build for all problems (fvm2d_precision); uploaded states are kept. */
+int fvm2d_batch_set_precision(fvm2d_batch *b, int precision);
+
+/* State of problem p in and out, as fvm2d_set_state / fvm2d_get_state. */
+int fvm2d_batch_set_state(fvm2d_batch *b, int p, const double *cells, int stride);
+int fvm2d_batch_get_state(fvm2d_batch *b, int p, double *cells, int stride);
+
+/* Runs every problem from t = 0 to its end time (solve() of each,
+ * src/wrappers.cuh:154-306, all at once). */
+int fvm2d_batch_solve(fvm2d_batch *b);
+
+/* Time reached and steps taken by problem p in the last solve. */
+int fvm2d_batch_get_time(fvm2d_batch *b, int p, double *t, int *steps);
+
+/* CUDA-event time of the last solve, kernels launched, and cell updates done
+ * (sum over problems of nx * ny * steps). */
+int fvm2d_batch_get_run_stats(fvm2d_batch *b, double *device_ms, long long *kernel_launches,
+                              long long *cell_updates);
+
+/* Times trial_steps steps of the batch for each candidate y-sweep segment
+ * length (16, 32, 64 interfaces) and sweep grid size (1, 2, 4 times the
+ * resident blocks), keeps the fastest and restores the states; reports the
+ * choice. */
+int fvm2d_batch_autotune(fvm2d_batch *b, int trial_steps, int *segment_interfaces, int *grid_blocks);
+
 /* Largest nx * ny that fvm2d_advance_noalloc accepts. */
 #define FVM2D_NOALLOC_MAX_CELLS 262144
 
