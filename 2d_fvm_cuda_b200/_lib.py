@@ -44,6 +44,10 @@ SIGNATURES = [
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
     ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_set_fixed_dt", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_jvp", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
+    ("fvm2d_forward", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("fvm2d_vjp", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     ("fvm2d_batch_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_batch_destroy", ctypes.c_int, [_vp]),
@@ -189,6 +193,27 @@ class Handle:
         k = ctypes.c_int(0)
         check(self.lib.fvm2d_profile_kernels(self.h, int(nsteps), out, ctypes.byref(k)))
         return list(out), k.value
+
+    # -- differentiation (fixed dt, FP64 build) --
+    def set_fixed_dt(self, dt: float) -> None:
+        check(self.lib.fvm2d_set_fixed_dt(self.h, float(dt)))
+
+    def jvp(self, nsteps: int, tangent) -> np.ndarray:
+        """Advances nsteps carrying `tangent`; returns the final tangent."""
+        T = as_cells(tangent)
+        out = np.empty((self.ny, self.nx, T.shape[2]))
+        check(self.lib.fvm2d_jvp(self.h, int(nsteps), T.ctypes.data, out.ctypes.data, T.shape[2]))
+        return out
+
+    def forward(self, nsteps: int, checkpoints: int) -> None:
+        check(self.lib.fvm2d_forward(self.h, int(nsteps), int(checkpoints)))
+
+    def vjp(self, cotangent) -> np.ndarray:
+        """Cotangent of the initial state of the last forward() for `cotangent` of its final state."""
+        C = as_cells(cotangent)
+        out = np.empty((self.ny, self.nx, C.shape[2]))
+        check(self.lib.fvm2d_vjp(self.h, C.ctypes.data, out.ctypes.data, C.shape[2]))
+        return out
 
     def time_stages_count(self) -> int:
         c = ctypes.c_longlong(0)

@@ -139,6 +139,7 @@ struct fvm2d_batch {
             q.plan.t_end = t_end[p];
             q.plan.cfl = cfl[p];
             q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
+            q.plan.fixed_dt = 0.0;
             q.nsegx = (nx[p] - 4 + 29) / 30;
             q.ncw = (nx[p] + 31) / 32;
             q.T = T;

@@ -11,7 +11,9 @@
 //   is one 64-byte read per graph replay (the reference reads the max wave
 //   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
 #include "../../include/fvm2d.h"
+#include "fvm2d_adjoint.h"
 #include "fvm2d_control.h"
+#include "fvm2d_dual.cuh"
 #include "fvm2d_transfer.cuh"
 
 #include <chrono>
@@ -20,6 +22,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 using fvm2d::LaunchConfig;
@@ -65,6 +68,26 @@ const Variant kVariants[] = {
      fvm2d::fp64_reforder::enqueue_step},
     {fvm2d::fp32::prepare, fvm2d::fp32::enqueue_init, fvm2d::fp32::enqueue_plan, fvm2d::fp32::enqueue_step},
 };
+// the tangent-linear build (dual numbers), used by fvm2d_jvp only
+const Variant kJvp = {fvm2d::jvp::prepare, fvm2d::jvp::enqueue_init, fvm2d::jvp::enqueue_plan,
+                      fvm2d::jvp::enqueue_step};
+
+using fvm2d::ad::Dual;
+
+// (value planes, tangent planes) <-> dual planes
+__global__ void pack_dual(const double *__restrict__ v, const double *__restrict__ t, Dual *__restrict__ out, long long n)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        out[k] = Dual(v[k], t[k]);
+}
+
+__global__ void unpack_dual(const Dual *__restrict__ in, double *__restrict__ v, double *__restrict__ t, long long n)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        v[k] = in[k].v;
+        t[k] = in[k].d;
+    }
+}
 
 // Element type of the state planes for a precision: FP32 stores floats, the
 // FP64 builds doubles.  Host-side states are always doubles.
@@ -94,6 +117,14 @@ struct fvm2d_solver {
     int graph_variant = -1;
     bool have_state = false;
     bool need_init = true;
+    double fixed_dt = 0.0;        // > 0: differentiation runs step with this constant dt
+    // differentiation workspaces (allocated on first use)
+    void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
+    double *ckpt = nullptr;       // checkpoints of fvm2d_forward
+    double *seg = nullptr;        // states of one segment, recomputed by fvm2d_vjp
+    double *adj = nullptr;        // adjoint work: 2 adjoints + 13 work states + saved final state
+    int ck_count = 0, ck_len = 0, ck_cap = 0, seg_cap = 0, fwd_steps = -1;
+    std::vector<double> ck_t;     // time at each checkpoint
     double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
     double last_device_ms = 0.0;  // CUDA-event time of the last loop on the stream
     long long last_launches = 0;  // kernels launched by the last loop
@@ -121,6 +152,7 @@ struct fvm2d_solver {
         c.plan.t_end = t_end;
         c.plan.cfl = cfl;
         c.plan.hmin = (c.hy < c.hx) ? c.hy : c.hx;
+        c.plan.fixed_dt = fixed_dt;
         return c;
     }
 
@@ -289,6 +321,10 @@ int fvm2d_destroy(fvm2d_solver *s)
     if (s->scratch) cudaFree(s->scratch);
     if (s->ctl) cudaFree(s->ctl);
     if (s->ctl_h) cudaFreeHost(s->ctl_h);
+    if (s->dual) cudaFree(s->dual);
+    if (s->ckpt) cudaFree(s->ckpt);
+    if (s->seg) cudaFree(s->seg);
+    if (s->adj) cudaFree(s->adj);
     if (s->ev_begin) cudaEventDestroy(s->ev_begin);
     if (s->ev_end) cudaEventDestroy(s->ev_end);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -513,6 +549,198 @@ int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *s
     s->total_steps += done;
     for (int q = 0; q < fvm2d::kStepKernels; ++q) kernel_ms[q] = done ? acc[q] / done : 0.0;
     if (steps_done) *steps_done = done;
+    return FVM2D_OK;
+}
+
+// ---- differentiation -------------------------------------------------------
+
+int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt)
+{
+    if (int rc = check(s)) return rc;
+    if (!(dt >= 0.0)) return fail(FVM2D_ERR_INVALID, "dt must be non-negative");
+    s->fixed_dt = dt;
+    s->fwd_steps = -1;
+    s->drop_graph();
+    return FVM2D_OK;
+}
+
+static int diff_ready(fvm2d_solver *s)
+{
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (s->precision != FVM2D_FP64) return fail(FVM2D_ERR_INVALID, "differentiation runs on the FP64 build (FVM2D_FP64)");
+    if (!(s->fixed_dt > 0.0)) return fail(FVM2D_ERR_INVALID, "set a fixed step size first (fvm2d_set_fixed_dt)");
+    return FVM2D_OK;
+}
+
+// Copies host or device cells (stride doubles) into 4 double planes at dst,
+// staging through the sweep buffers.
+static int cells_to_planes(fvm2d_solver *s, const double *cells, int stride, double *dst)
+{
+    const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
+    const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
+    aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, dst, s->nx, s->ny, s->pitch, s->plane);
+    CK(cudaGetLastError());
+    return FVM2D_OK;
+}
+
+static int planes_to_cells(fvm2d_solver *s, const double *src, double *cells, int stride)
+{
+    soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(src, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    CK(cudaGetLastError());
+    const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
+    const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(cells, s->scratch, bytes, kind, s->stream));
+    return FVM2D_OK;
+}
+
+int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tangent_out, int stride)
+{
+    if (int rc = check(s)) return rc;
+    if (int rc = diff_ready(s)) return rc;
+    if (!tangent_in || !tangent_out) return fail(FVM2D_ERR_INVALID, "null tangent pointer");
+    if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
+    if (nsteps < 0) return fail(FVM2D_ERR_INVALID, "nsteps must be non-negative");
+    const long long n4 = 4 * s->plane;
+    if (!s->dual) CK(cudaMalloc(&s->dual, 3 * n4 * sizeof(Dual)));
+    Dual *dU = static_cast<Dual *>(s->dual), *dA = dU + n4, *dB = dA + n4;
+    double *T = reinterpret_cast<double *>(dB);  // tangent planes, before packing and after unpacking
+    if (int rc = cells_to_planes(s, tangent_in, stride, T)) return rc;
+    pack_dual<<<148 * 4, 256, 0, s->stream>>>(s->U, T, dU, n4);
+    CK(cudaGetLastError());
+    LaunchConfig c = s->config();
+    c.U = dU;
+    c.A = dA;
+    c.B = dB;
+    StepControl *h = s->ctl_h;
+    const int before = h->steps;
+    h->step_limit = before + nsteps;
+    h->done = 0;
+    h->active = 0;
+    if (int rc = s->upload_control()) return rc;
+    CK(kJvp.init(c, s->stream));
+    for (int k = 0; k < nsteps; ++k) CK(kJvp.step(c, s->stream, nullptr));
+    CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+    unpack_dual<<<148 * 4, 256, 0, s->stream>>>(dU, s->U, T, n4);
+    CK(cudaGetLastError());
+    if (int rc = planes_to_cells(s, T, tangent_out, stride)) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    s->need_init = true;  // the state changed outside the FP64 graphs' bookkeeping
+    s->total_steps += h->steps - before;
+    s->fwd_steps = -1;
+    return FVM2D_OK;
+}
+
+int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
+{
+    if (int rc = check(s)) return rc;
+    if (int rc = diff_ready(s)) return rc;
+    if (nsteps < 1 || checkpoints < 1) return fail(FVM2D_ERR_INVALID, "nsteps and checkpoints must be positive");
+    if (checkpoints > nsteps) checkpoints = nsteps;
+    const int len = (nsteps + checkpoints - 1) / checkpoints;
+    const int count = (nsteps + len - 1) / len;
+    const long long n4 = 4 * s->plane;
+    if (count > s->ck_cap) {
+        if (s->ckpt) cudaFree(s->ckpt);
+        s->ckpt = nullptr;
+        s->ck_cap = 0;
+        CK(cudaMalloc(&s->ckpt, (size_t)count * n4 * sizeof(double)));
+        s->ck_cap = count;
+    }
+    StepControl *h = s->ctl_h;
+    h->step_limit = INT_MAX;
+    h->done = 0;
+    h->active = 0;
+    if (int rc = s->upload_control()) return rc;
+    const LaunchConfig c = s->config();
+    CK(s->need_init ? kVariants[FVM2D_FP64].init(c, s->stream) : kVariants[FVM2D_FP64].plan(c, s->stream));
+    s->need_init = false;
+    s->ck_t.assign(count, 0.0);
+    double t = h->t;
+    for (int k = 0; k < count; ++k) {
+        s->ck_t[k] = t;
+        CK(cudaMemcpyAsync(s->ckpt + k * n4, s->U, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        const int m = (k + 1) * len <= nsteps ? len : nsteps - k * len;
+        for (int j = 0; j < m; ++j) {
+            CK(kVariants[FVM2D_FP64].step(c, s->stream, nullptr));
+            t = t + s->fixed_dt;  // the same addition the device does
+        }
+    }
+    CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->ck_count = count;
+    s->ck_len = len;
+    s->fwd_steps = nsteps;
+    s->total_steps += nsteps;
+    return FVM2D_OK;
+}
+
+int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out, int stride)
+{
+    if (int rc = check(s)) return rc;
+    if (int rc = diff_ready(s)) return rc;
+    if (s->fwd_steps < 0) return fail(FVM2D_ERR_STATE, "fvm2d_vjp reverses the last fvm2d_forward: call it first");
+    if (!cotangent_in || !cotangent_out) return fail(FVM2D_ERR_INVALID, "null cotangent pointer");
+    if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
+    const long long n4 = 4 * s->plane;
+    const size_t sb = n4 * sizeof(double);
+    if (s->ck_len > s->seg_cap) {
+        if (s->seg) cudaFree(s->seg);
+        s->seg = nullptr;
+        s->seg_cap = 0;
+        CK(cudaMalloc(&s->seg, (size_t)s->ck_len * sb));
+        s->seg_cap = s->ck_len;
+    }
+    constexpr int kAdjStates = 16;  // two adjoints, 6 step work states, 7 sweep work states, the saved final state
+    if (!s->adj) CK(cudaMalloc(&s->adj, kAdjStates * sb));
+    double *lam = s->adj, *lam2 = s->adj + n4, *saved = s->adj + 15 * n4;
+    fvm2d::AdjointLaunch L;
+    L.nx = s->nx;
+    L.ny = s->ny;
+    L.pitch = s->pitch;
+    L.plane = s->plane;
+    L.strategy = s->strategy;
+    const LaunchConfig c = s->config();
+    L.hx = c.hx;
+    L.hy = c.hy;
+    L.rhx = c.rhx;
+    L.rhy = c.rhy;
+    L.alpha = s->alpha;
+    L.gamma = s->gamma;
+    L.dt = s->fixed_dt;
+    for (int k = 0; k < 6; ++k) L.state[k] = s->adj + (2 + k) * n4;
+    for (int k = 0; k < 7; ++k) L.work[k] = s->adj + (8 + k) * n4;
+    const StepControl after = *s->ctl_h;
+    CK(cudaMemcpyAsync(saved, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+    if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
+    StepControl *h = s->ctl_h;
+    for (int k = s->ck_count - 1; k >= 0; --k) {
+        const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
+        // recompute the segment from its checkpoint, keeping the input of every step
+        CK(cudaMemcpyAsync(s->U, s->ckpt + k * n4, sb, cudaMemcpyDeviceToDevice, s->stream));
+        std::memset(h, 0, sizeof(StepControl));
+        h->t = s->ck_t[k];
+        h->step_limit = INT_MAX;
+        if (int rc = s->upload_control()) return rc;
+        CK(kVariants[FVM2D_FP64].plan(c, s->stream));
+        for (int j = 0; j < m; ++j) {
+            CK(cudaMemcpyAsync(s->seg + j * n4, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+            if (j + 1 < m) CK(kVariants[FVM2D_FP64].step(c, s->stream, nullptr));
+        }
+        // reverse through the segment
+        for (int j = m - 1; j >= 0; --j) {
+            L.U = s->seg + j * n4;
+            L.lb_out = lam;
+            L.lb_in = lam2;
+            CK(fvm2d::adjoint_step(L, s->stream));
+            std::swap(lam, lam2);
+        }
+    }
+    if (int rc = planes_to_cells(s, lam, cotangent_out, stride)) return rc;
+    CK(cudaMemcpyAsync(s->U, saved, sb, cudaMemcpyDeviceToDevice, s->stream));
+    *h = after;
+    if (int rc = s->upload_control()) return rc;
+    CK(cudaStreamSynchronize(s->stream));
     return FVM2D_OK;
 }
 

@@ -22,9 +22,10 @@ struct StepControl {
 };
 
 struct PlanParams {
-    double t_end;  // end time
-    double cfl;    // CFL number
-    double hmin;   // min(width/nx, height/ny), wrappers.cuh:202
+    double t_end;     // end time
+    double cfl;       // CFL number
+    double hmin;      // min(width/nx, height/ny), wrappers.cuh:202
+    double fixed_dt;  // > 0: every step uses this dt (no CFL rule), for differentiation
 };
 
 // Everything one build of the kernels needs to enqueue a step.
@@ -44,7 +45,7 @@ struct LaunchConfig {
 constexpr int kStepKernels = 5;
 
 // The entry points each build of the kernels provides (namespaces fp64,
-// fp64_strict, fp64_reforder, fp32).
+// fp64_strict, fp64_reforder, fp32, and jvp: FP64 values with tangents).
 #define FVM2D_DECLARE_VARIANT(ns)                                              \
     namespace ns {                                                             \
     cudaError_t prepare();                                                     \
@@ -57,6 +58,7 @@ FVM2D_DECLARE_VARIANT(fp64)
 FVM2D_DECLARE_VARIANT(fp64_strict)
 FVM2D_DECLARE_VARIANT(fp64_reforder)
 FVM2D_DECLARE_VARIANT(fp32)
+FVM2D_DECLARE_VARIANT(jvp)
 
 // Records `msg` as the calling thread's fvm2d_last_error() text; returns code.
 int report_error(int code, const char *msg);

@@ -33,11 +33,18 @@ namespace FVM2D_VARIANT {
 
 // Start the next step if the loop of wrappers.cuh:196-207 continues:
 // dt = min(CFL h / smax, t_end - t); stop when t >= t_end or h/smax < 1e-20.
+// With a fixed step size (differentiation runs) dt is that constant and only
+// the step limit ends the loop.
 __device__ __forceinline__ void plan_step(StepControl *c, const PlanParams &p)
 {
     c->active = 0;
     if (c->done) return;
     if (c->steps >= c->step_limit) return;
+    if (p.fixed_dt > 0.0) {  // differentiation runs: a constant step size, bounded by the step count only
+        c->dt = p.fixed_dt;
+        c->active = 1;
+        return;
+    }
     const double t = c->t;
     if (!(t < p.t_end)) {
         c->done = 1;
@@ -197,14 +204,20 @@ __device__ __forceinline__ void store_cell(const Field<Real> &F, int x, int y, i
     F.at(ft, x, y) = c.ut;
 }
 
+// Value of the next (lane_down) or previous (lane_up) lane of the warp.
+__device__ __forceinline__ double lane_down(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float lane_down(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double lane_up(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float lane_up(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+
 template <typename Real>
 __device__ __forceinline__ Cell<Real> shfl_down(const Cell<Real> &c)
 {
     Cell<Real> o;
-    o.rho = __shfl_down_sync(0xffffffffu, c.rho, 1);
-    o.p = __shfl_down_sync(0xffffffffu, c.p, 1);
-    o.un = __shfl_down_sync(0xffffffffu, c.un, 1);
-    o.ut = __shfl_down_sync(0xffffffffu, c.ut, 1);
+    o.rho = lane_down(c.rho);
+    o.p = lane_down(c.p);
+    o.un = lane_down(c.un);
+    o.ut = lane_down(c.ut);
     return o;
 }
 
@@ -212,10 +225,10 @@ template <typename Real>
 __device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
 {
     Cell<Real> o;
-    o.rho = __shfl_up_sync(0xffffffffu, c.rho, 1);
-    o.p = __shfl_up_sync(0xffffffffu, c.p, 1);
-    o.un = __shfl_up_sync(0xffffffffu, c.un, 1);
-    o.ut = __shfl_up_sync(0xffffffffu, c.ut, 1);
+    o.rho = lane_up(c.rho);
+    o.p = lane_up(c.p);
+    o.un = lane_up(c.un);
+    o.ut = lane_up(c.ut);
     return o;
 }
 

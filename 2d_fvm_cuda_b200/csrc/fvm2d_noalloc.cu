@@ -133,6 +133,7 @@ int fvm2d_advance_noalloc(const double *state_in, double *state_out, int nx, int
     c.plan.t_end = t_end;
     c.plan.cfl = cfl;
     c.plan.hmin = (c.hy < c.hx) ? c.hy : c.hx;
+    c.plan.fixed_dt = 0.0;
 
     reset_control<<<1, 32, 0, s>>>(c.ctl, t0, nsteps);
     if ((e = cudaGetLastError())) return cuda_fail(e, "control reset");

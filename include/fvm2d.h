@@ -164,6 +164,33 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
  * fvm2d_advance.  No reference counterpart (diagnostics). */
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
 
+/* ---- differentiation (no reference counterpart) ----------------------------
+ * Derivatives of the FP64 step (FVM2D_FP64) with respect to the state, at a
+ * fixed step size so the CFL maximum is not differentiated.  Branches of the
+ * limiter and of the Riemann solver contribute the derivative of the branch
+ * taken (almost everywhere). */
+
+/* dt > 0: every step of this handle uses dt (no CFL rule; the run is bounded
+ * by its step count, not by the end time).  0 restores the reference's CFL
+ * rule. */
+int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt);
+
+/* Tangent-linear model: advances the state nsteps steps and carries the
+ * tangent (ny x nx cells of `stride` doubles) along; tangent_out receives the
+ * tangent of the final state.  Requires FVM2D_FP64 and a fixed dt. */
+int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tangent_out, int stride);
+
+/* Advances the state nsteps steps keeping `checkpoints` evenly spaced
+ * copies of it (sqrt(nsteps) is the usual choice) for fvm2d_vjp. */
+int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints);
+
+/* Adjoint of the last fvm2d_forward: given the cotangent of its final state,
+ * returns in cotangent_out the cotangent of its initial state (the
+ * vector-Jacobian product), recomputing each segment from its checkpoint and
+ * running the hand-written reverse step backwards through it.  The state and
+ * time are those after fvm2d_forward when it returns. */
+int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out, int stride);
+
 /* ---- batched form (no reference counterpart) -------------------------------
  * Many independent problems of different sizes advance together: every stage
  * of the step is one launch covering all problems, each problem with its own

@@ -1,0 +1,170 @@
+"""Differentiation form: tangent-linear (fvm2d_jvp) and adjoint (fvm2d_forward +
+fvm2d_vjp) of the FP64 step at fixed dt.
+
+The scheme is piecewise smooth: the limiter picks one of three differences
+or zero, the relaxation speeds take max(0, .), and the Riemann solver has wave
+cases.  On a uniform region all of these sit exactly on their switch (equal
+face states give a zero argument), where the tangent follows one branch and a
+central difference averages two.  Finite differences are therefore taken on
+data with no uniform region (large smooth waves in every field) or with
+perturbations small against the data's cell-to-cell differences, along smooth
+directions, so that only the few cells near an extremum or inflection line
+can cross a switch.
+
+* The JVP matches central finite differences of the forward on smooth data.
+* Dot-product test: <JVP(v), w> = <v, VJP(w)> for random v, w, over one step
+  and over many steps with checkpoints, on every ghost preset.
+* The gradient of J = sum (rho_T - rho_target)^2 with respect to the initial
+  density (the differentiation workload's objective, on a smaller array)
+  matches central finite differences.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def vortex_case(pkg, n, seed=3, amp=1e-3):
+    sc = pkg.scenarios
+    w, h, hh = sc.periodic_square_layout(n)
+    U = sc.isentropic_vortex(n, perturbation=sc.density_modes(16, amp, seed))
+    return U, w, h, hh
+
+
+def fixed_dt(pkg, U, hmin, gamma=1.4, cfl=0.45):
+    s = np.sqrt(U[..., 2] ** 2 + U[..., 3] ** 2) + np.sqrt(gamma * U[..., 1] / U[..., 0])
+    return cfl * hmin / s.max()
+
+
+def handle(pkg, U, width, height, dt, strategy=5):
+    ny, nx = U.shape[:2]
+    hd = pkg.Handle(nx, ny)
+    hd.configure(width, height, 1e9, 0.45, 1.9, 1.4, strategy, pkg.FP64)
+    hd.set_fixed_dt(dt)
+    hd.set_state(U)
+    return hd
+
+
+def forward(pkg, U, width, height, dt, steps, strategy=5):
+    hd = handle(pkg, U, width, height, dt, strategy)
+    hd.advance(steps)
+    V = hd.get_state(4)
+    hd.close()
+    return V
+
+
+def smooth_direction(pkg, n, seed):
+    """A smooth periodic perturbation of all four fields."""
+    sc = pkg.scenarios
+    _, _, h = sc.periodic_square_layout(n)
+    xs = (np.arange(n) - 2 + 0.5) * h
+    X, Y = np.meshgrid(xs, 10.0 - xs)
+    v = np.zeros((n, n, 4))
+    for f in range(4):
+        v[..., f] = sc.density_modes(6, 1.0, seed * 10 + f)(X, Y)
+    return v
+
+
+def waves(pkg, n):
+    """Periodic state with large smooth waves in every field, varying along both
+    directions (no field is uniform along a sweep line)."""
+    sc = pkg.scenarios
+    w, h, hh = sc.periodic_square_layout(n)
+    xs = (np.arange(n) - 2 + 0.5) * hh
+    X, Y = np.meshgrid(xs, 10.0 - xs)
+    k = 2 * np.pi / 10.0
+    U = np.empty((n, n, 4))
+    U[..., 0] = 1.0 + 0.3 * np.sin(k * X + 0.3) * np.sin(k * Y + 1.1)
+    U[..., 1] = 1.0 + 0.2 * np.cos(k * X + 0.7) * np.sin(2 * k * Y + 0.2)
+    U[..., 2] = 0.5 + 0.3 * np.sin(k * Y + 0.4) + 0.2 * np.cos(k * X + 0.9)
+    U[..., 3] = -0.3 + 0.2 * np.cos(k * X + 1.3) + 0.15 * np.sin(k * Y + 2.0)
+    return U, w, h, hh
+
+
+def test_jvp_matches_finite_differences(pkg):
+    n = 64
+    U, w, h, hh = waves(pkg, n)
+    dt = fixed_dt(pkg, U, hh)
+    v = smooth_direction(pkg, n, 1)
+    hd = handle(pkg, U, w, h, dt)
+    jv = hd.jvp(10, v)
+    hd.close()
+    # measured on B200: relative L2 1.6e-8 at eps 1e-8; above it the error
+    # grows in proportion to eps (cells pushed across a limiter switch)
+    eps = 1e-8
+    fd = (forward(pkg, U + eps * v, w, h, dt, 10) - forward(pkg, U - eps * v, w, h, dt, 10)) / (2 * eps)
+    err = np.linalg.norm(jv - fd) / np.linalg.norm(fd)
+    assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2, 3, 4, 5, 6])
+def test_dot_product_one_step_every_preset(pkg, oracle, strategy):
+    n = 48
+    U = pkg.scenarios.seeded_four_quadrant(n, 40, 70 + strategy)
+    U = oracle.ghost(U, strategy)
+    dt = fixed_dt(pkg, U, 1.0 / n) * 0.5
+    rng = np.random.default_rng(strategy)
+    v = rng.standard_normal(U.shape)
+    wv = rng.standard_normal(U.shape)
+    hd = handle(pkg, U, 1.0, 40 / n, dt, strategy)
+    jv = hd.jvp(1, v)
+    hd.set_state(U)
+    hd.forward(1, 1)
+    vj = hd.vjp(wv)
+    hd.close()
+    a, b = np.sum(jv * wv), np.sum(v * vj)
+    assert abs(a - b) <= 1e-11 * max(abs(a), abs(b)), (a, b)
+
+
+@pytest.mark.parametrize("steps,checkpoints", [(12, 4), (25, 5), (7, 1)])
+def test_dot_product_many_steps_with_checkpoints(pkg, steps, checkpoints):
+    U, w, h, hh = vortex_case(pkg, 96)
+    dt = fixed_dt(pkg, U, hh)
+    rng = np.random.default_rng(steps)
+    v = rng.standard_normal(U.shape)
+    wv = rng.standard_normal(U.shape)
+    hd = handle(pkg, U, w, h, dt)
+    jv = hd.jvp(steps, v)
+    final_jvp = hd.get_state(4)
+    hd.set_state(U)
+    hd.forward(steps, checkpoints)
+    final = hd.get_state(4)
+    # the dual-number build evaluates the same arithmetic in another kernel:
+    # both runs end in the same state up to FMA-contraction rounding
+    assert np.allclose(final, final_jvp, rtol=1e-12, atol=0)
+    vj = hd.vjp(wv)
+    assert np.array_equal(hd.get_state(4), final)  # the reverse leaves the final state in place
+    hd.close()
+    a, b = np.sum(jv * wv), np.sum(v * vj)
+    assert abs(a - b) <= 1e-10 * max(abs(a), abs(b)), (a, b)
+
+
+def test_gradient_of_density_objective_matches_finite_differences(pkg):
+    """J = sum (rho_T - rho_target)^2; the gradient with respect to the initial
+    density from fvm2d_vjp against central differences along random density
+    directions."""
+    n, steps = 128, 40
+    U, w, h, hh = vortex_case(pkg, n, seed=3)
+    Ut, _, _, _ = vortex_case(pkg, n, seed=11)
+    dt = fixed_dt(pkg, U, hh)
+    target = forward(pkg, Ut, w, h, dt, steps)[..., 0]
+
+    import math
+
+    def J(U0):  # summed accurately: the finite difference cancels most of it
+        return math.fsum(((forward(pkg, U0, w, h, dt, steps)[..., 0] - target) ** 2).ravel())
+
+    hd = handle(pkg, U, w, h, dt)
+    hd.forward(steps, int(np.ceil(np.sqrt(steps))))
+    UT = hd.get_state(4)
+    cot = np.zeros_like(U)
+    cot[..., 0] = 2 * (UT[..., 0] - target)
+    grad = hd.vjp(cot)[..., 0]
+    hd.close()
+    for k in range(3):
+        d = np.zeros_like(U)
+        d[..., 0] = smooth_direction(pkg, n, 20 + k)[..., 0]
+        eps = 1e-8  # small against the density modes' cell-to-cell differences (~1e-4)
+        fd = (J(U + eps * d) - J(U - eps * d)) / (2 * eps)
+        ad = np.sum(grad * d[..., 0])
+        assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
