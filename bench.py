@@ -361,6 +361,151 @@ def reference_arm(args, rank, world):
     }
 
 
+# ---------------------------------------------------------------------------
+# The north star's other forms, each printed as its own JSON line.
+# ---------------------------------------------------------------------------
+def form_batch(args):
+    """Batched form: 256 seeded four-quadrant problems, per-side size from
+    {128, 192, ..., 1024}, split point ~U[0.3, 0.7]^2, t_end 0.2, each with its
+    own CFL dt; one launch per stage over all problems (graph-captured loop)
+    against 256 sequential solves with the same build."""
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    sc = pkg.scenarios
+    spec = sc.uneven_batch(256, 3)
+    out = {"form": "batch", "workload": "256 four-quadrant problems, sides 128..1024, t_end 0.2", "results": []}
+    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32")):
+        b = pkg.Batch([(n, m) for n, m, _, _ in spec])
+        b.set_precision(prec)
+        for p, (n, m, seed, split) in enumerate(spec):
+            b.set_problem(p, 1.0, 1.0, 0.2, 0.45, 1.9, 1.4, 0)
+            b.set_state(p, sc.seeded_four_quadrant(n, m, seed, split))
+        T, g = b.autotune(2)
+        b.solve()
+        bms, launches, cu = b.run_stats()
+        finals = [b.get_state(p) for p in range(len(spec))]
+        b.close()
+        seq_ms, worst = 0.0, 0.0
+        for p, (n, m, seed, split) in enumerate(spec):
+            h = pkg.Handle(n, m)
+            h.configure(1.0, 1.0, 0.2, 0.45, 1.9, 1.4, 0, prec)
+            h.set_state(sc.seeded_four_quadrant(n, m, seed, split))
+            h.solve()
+            seq_ms += h.run_stats()[0]
+            V = h.get_state(4)
+            h.close()
+            worst = max(worst, max(float(np.nansum(np.abs(finals[p][..., f] - V[..., f])) /
+                                         np.nansum(np.abs(V[..., f]))) for f in range(4)))
+        out["results"].append({"precision": name, "cell_updates": cu, "batch_s": bms / 1e3,
+                               "batch_cell_updates_per_s": cu / (bms / 1e3), "sequential_s": seq_ms / 1e3,
+                               "sequential_cell_updates_per_s": cu / (seq_ms / 1e3), "speedup": seq_ms / bms,
+                               "autotuned": {"y_segment_interfaces": T, "grid_blocks": g},
+                               "max_rel_l1_vs_sequential": worst, "gpu_launches": launches})
+    return out
+
+
+def form_adjoint(args):
+    """Differentiation form: 512^2 periodic [0,10]^2, isentropic vortex plus 16
+    seeded density modes (amplitude <= 1e-3), fixed CFL-safe dt, 200 steps,
+    J = sum (rho_T - rho_target)^2 with the target from a second seeded
+    perturbation, gradient by fvm2d_vjp with ceil(sqrt(200)) = 15 checkpoints."""
+    import math
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    sc = pkg.scenarios
+    n, steps, ck = 512, 200, 15
+    w, hgt, hh = sc.periodic_square_layout(n)
+    U = sc.isentropic_vortex(n, perturbation=sc.density_modes(16, 1e-3, 3))
+    Ut = sc.isentropic_vortex(n, perturbation=sc.density_modes(16, 1e-3, 11))
+    speed = np.sqrt(U[..., 2] ** 2 + U[..., 3] ** 2) + np.sqrt(1.4 * U[..., 1] / U[..., 0])
+    dt = 0.45 * hh / speed.max()
+    h = pkg.Handle(n, n)
+    h.configure(w, hgt, 1e9, 0.45, 1.9, 1.4, 5, pkg.FP64)
+    h.set_fixed_dt(dt)
+
+    def run(U0):
+        h.set_state(U0)
+        h.advance(steps)
+        return h.get_state(4), h.run_stats()[0]
+
+    target = run(Ut)[0][..., 0]
+    run(U)  # warm
+    fwd_ms = min(run(U)[1] for _ in range(3))
+    import time
+    h.set_state(U)
+    t0 = time.perf_counter()
+    h.forward(steps, ck)
+    import ctypes  # noqa: F401
+    UT = h.get_state(4)
+    cot = np.zeros_like(U)
+    cot[..., 0] = 2 * (UT[..., 0] - target)
+    t1 = time.perf_counter()
+    grad = h.vjp(cot)[..., 0]
+    t2 = time.perf_counter()
+    # device-timed: forward with checkpoints + reverse, through CUDA events around both calls
+    import torch
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    h.set_state(U)
+    torch.cuda.synchronize()
+    e0.record()
+    h.forward(steps, ck)
+    e1.record()
+    h.vjp(cot)
+    e2.record()
+    torch.cuda.synchronize()
+    ck_ms, vjp_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    def J(U0):
+        return math.fsum(((run(U0)[0][..., 0] - target) ** 2).ravel())
+
+    xs = (np.arange(n) - 2 + 0.5) * hh
+    X, Y = np.meshgrid(xs, 10.0 - xs)
+    d = np.zeros_like(U)
+    d[..., 0] = sc.density_modes(6, 1.0, 20)(X, Y)
+    eps = 1e-8
+    fd = (J(U + eps * d) - J(U - eps * d)) / (2 * eps)
+    ad = float(np.sum(grad * d[..., 0]))
+    h.close()
+    return {"form": "adjoint", "workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, 15 checkpoints",
+            "forward_ms": fwd_ms, "forward_with_checkpoints_ms": ck_ms, "vjp_ms": vjp_ms,
+            "forward_plus_adjoint_over_forward": (ck_ms + vjp_ms) / fwd_ms,
+            "fd_check": {"direction": "6 smooth density modes", "eps": eps, "fd": fd, "adjoint": ad,
+                         "rel_diff": abs(fd - ad) / abs(ad)},
+            "wall_s": {"forward": t1 - t0, "vjp": t2 - t1}}
+
+
+def form_vortex(args):
+    """Isentropic vortex of strength 5 on periodic [0,10]^2, 2000^2 array,
+    background (1,1,1,1), advected one period (t_end 10), CFL 0.45: FP64 and
+    FP32 error against the exact (translated) vortex and FP32 against FP64."""
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    sc = pkg.scenarios
+    n = 2000
+    w, hgt, hh = sc.periodic_square_layout(n)
+    U0 = sc.isentropic_vortex(n)
+    res = {}
+    states = {}
+    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32")):
+        h = pkg.Handle(n, n)
+        h.configure(w, hgt, 10.0, 0.45, 1.9, 1.4, 5, prec)
+        h.set_state(U0)
+        h.solve()
+        ms, _ = h.run_stats()
+        t, steps, _ = h.time()
+        states[name] = h.get_state(4)
+        h.close()
+        res[name] = {"steps": steps, "t": t, "device_s": ms / 1e3, "cell_updates_per_s": n * n * steps / (ms / 1e3)}
+    E = sc.isentropic_vortex(n, t=res["fp64"]["t"])
+    inner = (slice(2, n - 2), slice(2, n - 2))
+
+    def rl1(A, B):
+        return float(np.abs(A[inner][..., 0] - B[inner][..., 0]).sum() / np.abs(B[inner][..., 0]).sum())
+
+    res["fp64"]["rho_rel_l1_vs_exact"] = rl1(states["fp64"], E)
+    res["fp32"]["rho_rel_l1_vs_exact"] = rl1(states["fp32"], E)
+    res["fp32"]["rho_rel_l1_vs_fp64"] = rl1(states["fp32"], states["fp64"])
+    res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
+    return {"form": "vortex", "workload": "2000^2 periodic isentropic vortex, one period", "results": res}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,10 +515,17 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side incl. ghosts (profiling cases)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
+    ap.add_argument("--form", choices=["batch", "adjoint", "vortex"],
+                    help="measure one of the other forms instead (one JSON line, rank 0, one GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     rank, world, local_rank = rank_info()
+    if args.form:
+        if rank == 0:
+            print(json.dumps({"batch": form_batch, "adjoint": form_adjoint, "vortex": form_vortex}[args.form](args)),
+                  flush=True)
+        return
     if args.impl == "reference":
         out = reference_arm(args, rank, world)
     else:
