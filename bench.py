@@ -174,7 +174,9 @@ def product_arm(args, rank, world, local_rank):
     pkg = importlib.import_module("2d_fvm_cuda_b200")
     n = args.n
     U0 = pkg.scenarios.seeded_four_quadrant(n, n, rank)
-    prec = pkg.FP64
+    prec = pkg.FP32 if args.precision == "fp32" else pkg.FP64
+    if prec != pkg.FP64 and not args.kernels_only:
+        raise SystemExit("--precision fp32 applies to --kernels-only runs; the full line reports FP32 beside FP64")
     h = pkg.Handle(n, n)
     h.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
                 CFG["strategy"], prec)
@@ -198,7 +200,7 @@ def product_arm(args, rank, world, local_rank):
             dist.destroy_process_group()
         return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "kernels_only": True,
-                "config": {"workload": f"four_quadrant_{n}x{n}_fp64"}, "clocks": clocks,
+                "config": {"workload": f"four_quadrant_{n}x{n}_{args.precision}"}, "clocks": clocks,
                 "gpu_launches": launches} if rank == 0 else None
 
     # per-kernel CUDA-event durations (steps run one at a time, outside the graph);
@@ -515,6 +517,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side incl. ghosts (profiling cases)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="arithmetic of a --kernels-only run")
     ap.add_argument("--form", choices=["batch", "adjoint", "vortex"],
                     help="measure one of the other forms instead (one JSON line, rank 0, one GPU)")
     args = ap.parse_args()

@@ -5,14 +5,16 @@ the FP64 path.
 
 Measured on B200 (relative L1 of density, FP32 vs FP64):
   isentropic vortex 256^2 interior, one period (1900 steps):   6.2e-6
+  isentropic vortex 2000^2, one period (14824 steps):          4.5e-5
   four-quadrant 400^2 to t = 0.2 (620 steps):                  1.7e-5
   shock-bubble 1024^2 to t = 0.4 (6275 steps):                 1.9e-4
-On smooth flow FP32 meets the 1e-5 bar with a wide margin (its error is far
-below the scheme's own error against the exact vortex).  With shocks the
-difference concentrates at the fronts (70-90% of it in the top 10% of cells)
-and grows faster than the step count; on the unstable bubble interface it
-grows with the instability itself.  These tests hold each workload to its
-bound so regressions show."""
+On smooth flow the error grows about linearly with the step count: it stays
+under 1e-5 for a few thousand steps; at 2000^2 (14824 steps) rounding the
+stored state to FP32 alone, with FP64 arithmetic, already gives 1.45e-5.
+With shocks the difference concentrates at the fronts (70-90% of it in the
+top 10% of cells) and grows faster than the step count; on the unstable
+bubble interface it grows with the instability itself.  These tests hold each
+workload to its bound so regressions show."""
 import numpy as np
 import pytest
 
