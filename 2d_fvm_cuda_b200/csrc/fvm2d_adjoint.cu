@@ -3,24 +3,26 @@
 //
 // The step is U' = ghost((Y(X(U)) + X(Y(U))) / 2).  Its adjoint, given the
 // adjoint lb' of U', is
-//   Vb = ghost^T lb'           (ring values are copies of interior cells)
-//   A2b = B2b = Vb / 2
-//   A1b = Y^T(A1) A2b ;  UbA = X^T(U) A1b      (branch A)
-//   B1b = X^T(B1) B2b ;  UbB = Y^T(U) B1b      (branch B)
+//   H   = ghost^T lb' / 2      (ring values are copies of interior cells)
+//   A1b = Y^T(A1) H ;  UbA = X^T(U) A1b      (branch A, A1 = X(U))
+//   B1b = X^T(B1) H ;  UbB = Y^T(U) B1b      (branch B, B1 = Y(U))
 //   lb  = UbA + UbB
-// with A1 = X(U) and B1 = Y(U) recomputed from U.  The transpose of a sweep
-// runs as four gathers over the array, one thread per cell or interface of a
-// line, so no value is accumulated by more than one thread:
-//   1. interface fluxes F (forward)
-//   2. per cell: adjoint of the conservative update -> the cell's direct part
-//      and the adjoint mb of its post-update conserved vector
-//   3. per interface: flux adjoint Fb = lambda (mb_right - mb_left), then the
-//      adjoint of face states, relaxation GRP and midpoint flux -> adjoints of
-//      the two cells and the two slopes it used
-//   4. per cell: gather the direct part, the two interfaces' face-state parts
-//      and the limiter adjoint of the three slopes that read the cell
-// Only the ghost transpose adds with atomics (several ring cells may copy the
-// same interior cell).
+// A1, B1 and the interface fluxes of the four sweeps come from the forward
+// step's tape (fp64::enqueue_step_taped), so no forward sweep is rerun.
+//
+// A sweep's transpose is one kernel.  A warp holds 32 consecutive positions
+// of a line, one per lane, and does in registers, exchanging neighbours by
+// shuffles: the limited slope of its cell, the adjoint of its cell's
+// conservative update (from the taped fluxes), the adjoint of its interface
+// (face states, relaxation GRP and midpoint flux, recomputed forward and then
+// reversed), the limiter's adjoint of its slope, and finally the gather of
+// every part that reaches its cell.  An output depends on positions up to
+// three away, so lanes 3..28 (26 positions) are exact and work items overlap
+// by six positions; no value is accumulated by two threads.  x-lines are read
+// straight from global memory (coalesced along rows); y-lines go through a
+// shared-memory tile of 8 columns x 32 positions that is loaded and stored
+// row by row.  Only the ghost ring's transpose adds with atomics (several
+// ring cells may copy the same interior cell).
 #define FVM2D_VARIANT adj
 #include "fvm2d_adjoint_math.cuh"
 #include "fvm2d_adjoint.h"
@@ -29,47 +31,10 @@
 namespace fvm2d {
 namespace adj {
 
-using Phys = Hoisted;
-constexpr int ANT = 256;
-
-struct SweepGeom {
-    int nx, ny, dir;  // dir 0: x-sweep; 1: y-sweep (line position l = ny-1-j, (un, ut) = (v, u))
-    __device__ __forceinline__ int L() const { return dir == 0 ? nx : ny; }
-    __device__ __forceinline__ int NC() const { return dir == 0 ? ny : nx; }
-    __device__ __forceinline__ int x(int l, int c) const { return dir == 0 ? l : c; }
-    __device__ __forceinline__ int y(int l, int c) const { return dir == 0 ? c : ny - 1 - l; }
-    __device__ __forceinline__ int fn() const { return dir == 0 ? 2 : 3; }
-    __device__ __forceinline__ int ft() const { return dir == 0 ? 3 : 2; }
-};
-
-// (l, c) of this thread: lines run along threadIdx.x for x-sweeps so that
-// global accesses stay coalesced, across threadIdx.x for y-sweeps.
-__device__ __forceinline__ bool thread_lc(const SweepGeom &G, int &l, int &c)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    l = G.dir == 0 ? i : j;
-    c = G.dir == 0 ? j : i;
-    return l < G.L() && c < G.NC();
-}
-
-__device__ __forceinline__ Cell<A> ld(const Field<A> &F, const SweepGeom &G, int l, int c)
-{
-    return load_cell(F, G.x(l, c), G.y(l, c), G.fn(), G.ft());
-}
-__device__ __forceinline__ void st(const Field<A> &F, const SweepGeom &G, int l, int c, const Cell<A> &v)
-{
-    store_cell(F, G.x(l, c), G.y(l, c), G.fn(), G.ft(), v);
-}
-// flux-slot quantities (mass, normal momentum, energy, tangential momentum) are
-// stored in plane order 0..3 without the u/v mapping
-__device__ __forceinline__ Cell<A> ldf(const Field<A> &F, const SweepGeom &G, int l, int c)
-{
-    return load_cell(F, G.x(l, c), G.y(l, c), 2, 3);
-}
-__device__ __forceinline__ void stf(const Field<A> &F, const SweepGeom &G, int l, int c, const Cell<A> &v)
-{
-    store_cell(F, G.x(l, c), G.y(l, c), 2, 3, v);
-}
+constexpr int ANT = 128;         // threads per block of the sweep transposes
+constexpr int kLineOut = 26;     // exact positions per 32-lane item (lanes 3..28)
+constexpr int kTileCols = 8;     // columns of a y-line tile
+constexpr int kTileStride = kTileCols + 1;  // odd stride: conflict-free column reads
 
 __device__ __forceinline__ Cell<A> zero_cell() { return {0.0, 0.0, 0.0, 0.0}; }
 __device__ __forceinline__ Cell<A> add(const Cell<A> &a, const Cell<A> &b)
@@ -77,105 +42,124 @@ __device__ __forceinline__ Cell<A> add(const Cell<A> &a, const Cell<A> &b)
     return {a.rho + b.rho, a.p + b.p, a.un + b.un, a.ut + b.ut};
 }
 
-struct SweepParams {
-    SweepGeom G;
-    SweepConsts<A> K;
+// Adjoint of one sweep at line position c of a line of L cells, one position
+// per lane: U is the cell swept, ub the adjoint of the sweep's output there,
+// F the taped flux of interface c-1/2 (zero where c is not an interface).
+// Returns the adjoint of the sweep's input at c; exact on lanes 3..28.
+// Ranges follow the forward sweep: slopes 1..L-2, interfaces 2..L-2, updated
+// cells 2..L-3; the others pass through.
+__device__ __forceinline__ Cell<A> line_adjoint(const Cell<A> &U, const Cell<A> &ub, const Cell<A> &F, int c, int L,
+                                                const SweepConsts<A> &K)
+{
+    const Cell<A> Um = shfl_up(U), Up = shfl_down(U);
+    const bool has_slope = c >= 1 && c <= L - 2;
+    const bool iface = c >= 2 && c <= L - 2;
+    Cell<A> s = zero_cell();
+    if (has_slope) s = cell_slope(Um, U, Up, K);
+    const Cell<A> sm = shfl_up(s);
+    const Cell<A> FR = shfl_down(F);
+    // the cell's conservative update
+    Cell<A> r = zero_cell(), mb = zero_cell();
+    if (c >= 2 && c <= L - 3)
+        mb = update_adjoint(U, F, FR, K, ub, r);
+    else
+        r = ub;
+    const Cell<A> mbm = shfl_up(mb);
+    // interface c-1/2: the flux leaves cell c-1 (-lambda) and enters cell c (+lambda)
+    Cell<A> a = zero_cell(), b = zero_cell(), sa = zero_cell(), sb = zero_cell();
+    if (iface) {
+        const A lam = K.lambda;
+        const Cell<A> Fb = {lam * (mb.rho - mbm.rho), lam * (mb.p - mbm.p), lam * (mb.un - mbm.un),
+                            lam * (mb.ut - mbm.ut)};
+        interface_flux_adjoint(Um, U, sm, s, K, Fb, a, b, sa, sb);
+    }
+    r = add(r, b);                // right cell of interface c-1/2
+    r = add(r, shfl_down(a));     // left cell of interface c+1/2
+    // slope c: right slope of interface c-1/2, left slope of interface c+1/2
+    const Cell<A> sbar = add(sb, shfl_down(sa));
+    Cell<A> mbar = zero_cell(), cbar = zero_cell(), pbar = zero_cell();
+    if (has_slope) {
+        slope_adjoint(slope_choice(Um.rho, U.rho, Up.rho, K.rh, K.alpha), sbar.rho, K.rh, K.alpha, mbar.rho, cbar.rho,
+                      pbar.rho);
+        slope_adjoint(slope_choice(Um.p, U.p, Up.p, K.rh, K.alpha), sbar.p, K.rh, K.alpha, mbar.p, cbar.p, pbar.p);
+        slope_adjoint(slope_choice(Um.un, U.un, Up.un, K.rh, K.alpha), sbar.un, K.rh, K.alpha, mbar.un, cbar.un,
+                      pbar.un);
+        slope_adjoint(slope_choice(Um.ut, U.ut, Up.ut, K.rh, K.alpha), sbar.ut, K.rh, K.alpha, mbar.ut, cbar.ut,
+                      pbar.ut);
+    }
+    r = add(r, cbar);             // slope c
+    r = add(r, shfl_up(pbar));    // slope c-1 (this cell is its right cell)
+    r = add(r, shfl_down(mbar));  // slope c+1 (this cell is its left cell)
+    return r;
+}
+
+struct SweepT {
+    Field<A> U, F, ub, out, addend;  // addend.base may be null
+    int nx, ny;
+    adj::SweepConsts<A> K;
 };
 
-__device__ __forceinline__ Cell<A> slope_at(const Field<A> &U, const SweepParams &P, int l, int c)
+// out = X^T ub (+ addend).  Work item: row y, positions 26 seg - 3 .. 26 seg + 28.
+__global__ void __launch_bounds__(ANT, 2) adjoint_x_kernel(SweepT g)
 {
-    return cell_slope(ld(U, P.G, l - 1, c), ld(U, P.G, l, c), ld(U, P.G, l + 1, c), P.K);
-}
-
-// 1. interface fluxes: F(l) for the interface between cells l-1 and l
-__global__ void __launch_bounds__(ANT) flux_kernel(Field<A> U, Field<A> F, SweepParams P)
-{
-    int l, c;
-    if (!thread_lc(P.G, l, c) || l < 2 || l > P.G.L() - 2) return;
-    const Cell<A> sm = slope_at(U, P, l - 1, c), s0 = slope_at(U, P, l, c);
-    stf(F, P.G, l, c, Phys::interface_flux(ld(U, P.G, l - 1, c), ld(U, P.G, l, c), sm, s0, P.K));
-}
-
-// forward update of a sweep from the fluxes (recomputes A1 = X(U), B1 = Y(U))
-__global__ void __launch_bounds__(ANT) update_kernel(Field<A> U, Field<A> F, Field<A> out, SweepParams P)
-{
-    int l, c;
-    if (!thread_lc(P.G, l, c)) return;
-    const Cell<A> u = ld(U, P.G, l, c);
-    if (l >= 2 && l <= P.G.L() - 3)
-        st(out, P.G, l, c, Phys::update(u, ldf(F, P.G, l, c), ldf(F, P.G, l + 1, c), P.K));
-    else
-        st(out, P.G, l, c, u);
-}
-
-// 2. per cell: adjoint of the update
-__global__ void __launch_bounds__(ANT) update_adjoint_kernel(Field<A> U, Field<A> F, Field<A> Ub_out, Field<A> Up,
-                                                             Field<A> Mb, SweepParams P)
-{
-    int l, c;
-    if (!thread_lc(P.G, l, c)) return;
-    const Cell<A> ub = ld(Ub_out, P.G, l, c);
-    if (l >= 2 && l <= P.G.L() - 3) {
-        Cell<A> part = zero_cell();
-        const Cell<A> mb =
-            update_adjoint(ld(U, P.G, l, c), ldf(F, P.G, l, c), ldf(F, P.G, l + 1, c), P.K, ub, part);
-        st(Up, P.G, l, c, part);
-        stf(Mb, P.G, l, c, mb);
-    } else {  // pass-through cell
-        st(Up, P.G, l, c, ub);
-        stf(Mb, P.G, l, c, zero_cell());
-    }
-}
-
-// 3. per interface: adjoint of face states, GRP and flux
-__global__ void __launch_bounds__(ANT) interface_adjoint_kernel(Field<A> U, Field<A> Mb, Field<A> ULb, Field<A> URb,
-                                                                Field<A> sLb, Field<A> sRb, SweepParams P)
-{
-    int l, c;
-    if (!thread_lc(P.G, l, c) || l < 2 || l > P.G.L() - 2) return;
-    const Cell<A> mr = ldf(Mb, P.G, l, c), ml = ldf(Mb, P.G, l - 1, c);
-    const A lam = P.K.lambda;
-    // the interface is F_L of cell l (+lambda) and F_R of cell l-1 (-lambda)
-    const Cell<A> Fb = {lam * (mr.rho - ml.rho), lam * (mr.p - ml.p), lam * (mr.un - ml.un), lam * (mr.ut - ml.ut)};
-    const Cell<A> sm = slope_at(U, P, l - 1, c), s0 = slope_at(U, P, l, c);
-    Cell<A> a = zero_cell(), b = zero_cell(), sa = zero_cell(), sb = zero_cell();
-    interface_flux_adjoint(ld(U, P.G, l - 1, c), ld(U, P.G, l, c), sm, s0, P.K, Fb, a, b, sa, sb);
-    st(ULb, P.G, l, c, a);
-    st(URb, P.G, l, c, b);
-    st(sLb, P.G, l, c, sa);
-    st(sRb, P.G, l, c, sb);
-}
-
-// 4. per cell: gather every contribution to the adjoint of the sweep input
-__global__ void __launch_bounds__(ANT) gather_kernel(Field<A> U, Field<A> Up, Field<A> ULb, Field<A> URb,
-                                                     Field<A> sLb, Field<A> sRb, Field<A> Ub_in, SweepParams P)
-{
-    int l, c;
-    if (!thread_lc(P.G, l, c)) return;
-    const int L = P.G.L();
-    auto iface = [&](int j) { return j >= 2 && j <= L - 2; };
-    Cell<A> r = ld(Up, P.G, l, c);
-    if (iface(l)) r = add(r, ld(URb, P.G, l, c));          // right cell of interface l
-    if (iface(l + 1)) r = add(r, ld(ULb, P.G, l + 1, c));  // left cell of interface l+1
-    // slopes j = l-1, l, l+1 read this cell
-    for (int j = l - 1; j <= l + 1; ++j) {
-        if (j < 1 || j > L - 2) continue;
-        Cell<A> sb = zero_cell();
-        if (iface(j)) sb = add(sb, ld(sRb, P.G, j, c));          // slope j as the right slope of interface j
-        if (iface(j + 1)) sb = add(sb, ld(sLb, P.G, j + 1, c));  // ... and the left slope of interface j+1
-        const Cell<A> um = ld(U, P.G, j - 1, c), u0 = ld(U, P.G, j, c), up = ld(U, P.G, j + 1, c);
-        const A um4[4] = {um.rho, um.p, um.un, um.ut}, u04[4] = {u0.rho, u0.p, u0.un, u0.ut};
-        const A up4[4] = {up.rho, up.p, up.un, up.ut}, sb4[4] = {sb.rho, sb.p, sb.un, sb.ut};
-        A out[4] = {0, 0, 0, 0};
-        for (int f = 0; f < 4; ++f) {
-            A mb = 0, cb = 0, pb = 0;
-            slope_adjoint(slope_choice(um4[f], u04[f], up4[f], P.K.rh, P.K.alpha), sb4[f], P.K.rh, P.K.alpha, mb,
-                          cb, pb);
-            out[f] = (l == j - 1) ? mb : (l == j ? cb : pb);
+    const int lane = threadIdx.x & 31;
+    const int nseg = (g.nx + kLineOut - 1) / kLineOut;
+    const long long nwork = (long long)nseg * g.ny;
+    const long long wstride = (long long)gridDim.x * (ANT / 32);
+    for (long long w = (long long)blockIdx.x * (ANT / 32) + threadIdx.x / 32; w < nwork; w += wstride) {
+        const int y = int(w / nseg), seg = int(w % nseg);
+        const int c = kLineOut * seg + lane - 3;
+        const bool in = c >= 0 && c < g.nx;
+        const int xc = min(max(c, 0), g.nx - 1);
+        const Cell<A> U = load_cell(g.U, xc, y, 2, 3);
+        const Cell<A> ub = in ? load_cell(g.ub, xc, y, 2, 3) : zero_cell();
+        const Cell<A> F = (c >= 2 && c <= g.nx - 2) ? load_cell(g.F, c, y, 2, 3) : zero_cell();
+        Cell<A> r = line_adjoint(U, ub, F, c, g.nx, g.K);
+        if (lane >= 3 && lane <= 28 && in) {
+            if (g.addend.base) r = add(r, load_cell(g.addend, c, y, 2, 3));
+            store_cell(g.out, c, y, 2, 3, r);
         }
-        r = add(r, Cell<A>{out[0], out[1], out[2], out[3]});
     }
-    st(Ub_in, P.G, l, c, r);
+}
+
+// out = Y^T ub (+ addend).  Block: columns 8 bx .. 8 bx + 7, line positions
+// 26 by - 3 .. 26 by + 28 (position l is row ny-1-l; (un, ut) = (v, u)).
+__global__ void __launch_bounds__(ANT, 2) adjoint_y_kernel(SweepT g)
+{
+    __shared__ A sU[4][32][kTileStride], sB[4][32][kTileStride], sF[4][32][kTileStride];
+    const int x0 = blockIdx.x * kTileCols, l0 = blockIdx.y * kLineOut - 3;
+    const int nx = g.nx, ny = g.ny;
+    for (int q = threadIdx.x; q < 32 * kTileCols; q += ANT) {
+        const int k = q / kTileCols, col = q % kTileCols;
+        const int x = min(x0 + col, nx - 1), l = l0 + k;
+        const int j = ny - 1 - min(max(l, 0), ny - 1);
+        const Cell<A> U = load_cell(g.U, x, j, 3, 2);
+        const Cell<A> ub = (l >= 0 && l < ny) ? load_cell(g.ub, x, j, 3, 2) : zero_cell();
+        const Cell<A> F = (l >= 2 && l <= ny - 2) ? load_cell(g.F, x, j, 2, 3) : zero_cell();
+        sU[0][k][col] = U.rho; sU[1][k][col] = U.p; sU[2][k][col] = U.un; sU[3][k][col] = U.ut;
+        sB[0][k][col] = ub.rho; sB[1][k][col] = ub.p; sB[2][k][col] = ub.un; sB[3][k][col] = ub.ut;
+        sF[0][k][col] = F.rho; sF[1][k][col] = F.p; sF[2][k][col] = F.un; sF[3][k][col] = F.ut;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
+    for (int col = warp; col < kTileCols; col += ANT / 32) {
+        const Cell<A> U = {sU[0][lane][col], sU[1][lane][col], sU[2][lane][col], sU[3][lane][col]};
+        const Cell<A> ub = {sB[0][lane][col], sB[1][lane][col], sB[2][lane][col], sB[3][lane][col]};
+        const Cell<A> F = {sF[0][lane][col], sF[1][lane][col], sF[2][lane][col], sF[3][lane][col]};
+        const Cell<A> r = line_adjoint(U, ub, F, l0 + lane, ny, g.K);
+        // each warp owns its columns: the result replaces its own ub entry
+        sB[0][lane][col] = r.rho; sB[1][lane][col] = r.p; sB[2][lane][col] = r.un; sB[3][lane][col] = r.ut;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 32 * kTileCols; q += ANT) {
+        const int k = q / kTileCols, col = q % kTileCols;
+        const int x = x0 + col, l = l0 + k;
+        if (k < 3 || k > 28 || x >= nx || l >= ny) continue;
+        const int j = ny - 1 - l;
+        Cell<A> r = {sB[0][k][col], sB[1][k][col], sB[2][k][col], sB[3][k][col]};
+        if (g.addend.base) r = add(r, load_cell(g.addend, x, j, 3, 2));
+        store_cell(g.out, x, j, 3, 2, r);
+    }
 }
 
 // ---- ghost ring transpose ------------------------------------------------
@@ -252,17 +236,17 @@ __device__ __forceinline__ bool on_ring(const GhostGeom &g, int i, int j)
     return i < 2 || i >= g.nx - 2 || j < 2 || j >= g.ny - 2;
 }
 
-// Vb = lb with the ring zeroed
-__global__ void ghost_adjoint_copy(Field<A> lb, Field<A> Vb, GhostGeom g)
+// Vb = scale * lb with the ring zeroed
+__global__ void ghost_adjoint_copy(Field<A> lb, Field<A> Vb, GhostGeom g, A scale)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.nx || j >= g.ny) return;
     const bool ring = on_ring(g, i, j);
-    for (int f = 0; f < 4; ++f) Vb.at(f, i, j) = ring ? 0.0 : lb.at(f, i, j);
+    for (int f = 0; f < 4; ++f) Vb.at(f, i, j) = ring ? 0.0 : scale * lb.at(f, i, j);
 }
 
-// Vb(source) += sign * lb(ring cell)
-__global__ void ghost_adjoint_scatter(Field<A> lb, Field<A> Vb, GhostGeom g)
+// Vb(source) += scale * sign * lb(ring cell)
+__global__ void ghost_adjoint_scatter(Field<A> lb, Field<A> Vb, GhostGeom g, A scale)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int nrow = 4 * g.nx, ncol = 4 * (g.ny - 4);
@@ -280,18 +264,10 @@ __global__ void ghost_adjoint_scatter(Field<A> lb, Field<A> Vb, GhostGeom g)
     int si, sj;
     A vs;
     if (!ring_source(g.strategy, g.nx, g.ny, i, j, si, sj, vs)) return;
-    atomicAdd(&Vb.at(0, si, sj), lb.at(0, i, j));
-    atomicAdd(&Vb.at(1, si, sj), lb.at(1, i, j));
-    atomicAdd(&Vb.at(2, si, sj), lb.at(2, i, j));
-    atomicAdd(&Vb.at(3, si, sj), vs * lb.at(3, i, j));
-}
-
-// out = a * x + b * y over the 4 planes
-__global__ void axpby_kernel(Field<A> x, Field<A> y, Field<A> out, A a, A b, int nx, int ny)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= nx || j >= ny) return;
-    for (int f = 0; f < 4; ++f) out.at(f, i, j) = a * x.at(f, i, j) + b * y.at(f, i, j);
+    atomicAdd(&Vb.at(0, si, sj), scale * lb.at(0, i, j));
+    atomicAdd(&Vb.at(1, si, sj), scale * lb.at(1, i, j));
+    atomicAdd(&Vb.at(2, si, sj), scale * lb.at(2, i, j));
+    atomicAdd(&Vb.at(3, si, sj), scale * vs * lb.at(3, i, j));
 }
 
 } // namespace adj
@@ -301,87 +277,82 @@ namespace {
 
 using adj::A;
 
-adj::SweepParams sweep_params(const AdjointLaunch &L, int dir)
-{
-    adj::SweepParams P;
-    P.G.nx = L.nx;
-    P.G.ny = L.ny;
-    P.G.dir = dir;
-    const double h = dir == 0 ? L.hx : L.hy;
-    P.K.h = h;
-    P.K.rh = dir == 0 ? L.rhx : L.rhy;
-    P.K.alpha = L.alpha;
-    P.K.g = L.gamma;
-    P.K.k = L.dt;
-    P.K.lambda = L.dt / h;
-    P.K.igm1 = 1.0 / (L.gamma - 1.0);
-    P.K.kappa = (L.gamma + 1.0) / 2.0;
-    return P;
-}
-
-adj::Field<A> fld(double *p, const AdjointLaunch &L)
+adj::Field<A> fld(const double *p, const AdjointLaunch &L)
 {
     adj::Field<A> f;
-    f.base = p;
+    f.base = const_cast<double *>(p);
     f.plane = L.plane;
     f.pitch = L.pitch;
     return f;
 }
 
-dim3 sweep_grid(const AdjointLaunch &L, int dir)
+adj::SweepConsts<A> consts(const AdjointLaunch &L, int dir)
 {
-    const int L_ = dir == 0 ? L.nx : L.ny, NC = dir == 0 ? L.ny : L.nx;
-    // x-sweeps: lines along threadIdx.x; y-sweeps: cross index along threadIdx.x
-    return dir == 0 ? dim3((L_ + 31) / 32, (NC + 7) / 8) : dim3((NC + 31) / 32, (L_ + 7) / 8);
+    adj::SweepConsts<A> K;
+    const double h = dir == 0 ? L.hx : L.hy;
+    K.h = h;
+    K.rh = dir == 0 ? L.rhx : L.rhy;
+    K.alpha = L.alpha;
+    K.g = L.gamma;
+    K.k = L.dt;
+    K.lambda = L.dt / h;
+    K.igm1 = 1.0 / (L.gamma - 1.0);
+    K.kappa = (L.gamma + 1.0) / 2.0;
+    return K;
 }
 
-// out = sweep_dir(U)
-void forward_sweep(const AdjointLaunch &L, int dir, double *U, double *out, cudaStream_t s)
-{
-    const adj::SweepParams P = sweep_params(L, dir);
-    const dim3 g = sweep_grid(L, dir), b(32, 8);
-    adj::flux_kernel<<<g, b, 0, s>>>(fld(U, L), fld(L.work[0], L), P);
-    adj::update_kernel<<<g, b, 0, s>>>(fld(U, L), fld(L.work[0], L), fld(out, L), P);
-}
+int g_sms = 0, g_occ_x = 1;
 
-// Ub_in = (d sweep_dir / dU at U)^T Ub_out
-void adjoint_sweep(const AdjointLaunch &L, int dir, double *U, double *Ub_out, double *Ub_in, cudaStream_t s)
+// out = (d sweep_dir / dU at U)^T ub (+ addend)
+void sweep_transpose(const AdjointLaunch &L, int dir, const double *U, const double *F, const double *ub,
+                     double *out, const double *addend, cudaStream_t s)
 {
-    const adj::SweepParams P = sweep_params(L, dir);
-    const dim3 g = sweep_grid(L, dir), b(32, 8);
-    double *F = L.work[0], *Up = L.work[1], *Mb = L.work[2];
-    double *ULb = L.work[3], *URb = L.work[4], *sLb = L.work[5], *sRb = L.work[6];
-    adj::flux_kernel<<<g, b, 0, s>>>(fld(U, L), fld(F, L), P);
-    adj::update_adjoint_kernel<<<g, b, 0, s>>>(fld(U, L), fld(F, L), fld(Ub_out, L), fld(Up, L), fld(Mb, L), P);
-    adj::interface_adjoint_kernel<<<g, b, 0, s>>>(fld(U, L), fld(Mb, L), fld(ULb, L), fld(URb, L), fld(sLb, L),
-                                                  fld(sRb, L), P);
-    adj::gather_kernel<<<g, b, 0, s>>>(fld(U, L), fld(Up, L), fld(ULb, L), fld(URb, L), fld(sLb, L), fld(sRb, L),
-                                       fld(Ub_in, L), P);
+    adj::SweepT g;
+    g.U = fld(U, L);
+    g.F = fld(F, L);
+    g.ub = fld(ub, L);
+    g.out = fld(out, L);
+    g.addend = fld(addend, L);
+    g.nx = L.nx;
+    g.ny = L.ny;
+    g.K = consts(L, dir);
+    if (dir == 0) {
+        const long long items = (long long)((L.nx + adj::kLineOut - 1) / adj::kLineOut) * L.ny;
+        long long blocks = (items + adj::ANT / 32 - 1) / (adj::ANT / 32);
+        const long long cap = (long long)g_occ_x * g_sms;
+        adj::adjoint_x_kernel<<<int(blocks < cap ? blocks : cap), adj::ANT, 0, s>>>(g);
+    } else {
+        const dim3 grid((L.nx + adj::kTileCols - 1) / adj::kTileCols, (L.ny + adj::kLineOut - 1) / adj::kLineOut);
+        adj::adjoint_y_kernel<<<grid, adj::ANT, 0, s>>>(g);
+    }
 }
 
 } // namespace
 
 cudaError_t adjoint_step(const AdjointLaunch &L, cudaStream_t s)
 {
-    const dim3 g2((L.nx + 31) / 32, (L.ny + 7) / 8), b2(32, 8);
-    adj::GhostGeom gg{L.nx, L.ny, L.strategy};
-    double *A1 = L.state[0], *B1 = L.state[1], *H = L.state[2], *T1 = L.state[3], *T2 = L.state[4],
-           *T3 = L.state[5];
-    // recompute the first sweeps of both branches
-    forward_sweep(L, 0, L.U, A1, s);
-    forward_sweep(L, 1, L.U, B1, s);
+    if (!g_sms) {
+        int dev = 0;
+        cudaError_t e;
+        if ((e = cudaGetDevice(&dev))) return e;
+        if ((e = cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_x, adj::adjoint_x_kernel, adj::ANT, 0)))
+            return e;
+        if (g_occ_x < 1) g_occ_x = 1;
+    }
+    double *H = L.work[0], *T1 = L.work[1], *T2 = L.work[2];
     // ghost fill and average, transposed: H = ghost^T(lb_out) / 2
-    adj::ghost_adjoint_copy<<<g2, b2, 0, s>>>(fld(L.lb_out, L), fld(H, L), gg);
+    const dim3 g2((L.nx + 31) / 32, (L.ny + 7) / 8), b2(32, 8);
+    const adj::GhostGeom gg{L.nx, L.ny, L.strategy};
+    adj::ghost_adjoint_copy<<<g2, b2, 0, s>>>(fld(L.lb_out, L), fld(H, L), gg, 0.5);
     const int ring = 4 * L.nx + 4 * (L.ny - 4);
-    adj::ghost_adjoint_scatter<<<(ring + 255) / 256, 256, 0, s>>>(fld(L.lb_out, L), fld(H, L), gg);
-    adj::axpby_kernel<<<g2, b2, 0, s>>>(fld(H, L), fld(H, L), fld(H, L), 0.5, 0.0, L.nx, L.ny);
+    adj::ghost_adjoint_scatter<<<(ring + 255) / 256, 256, 0, s>>>(fld(L.lb_out, L), fld(H, L), gg, 0.5);
     // branch A: A2 = Y(A1), A1 = X(U)
-    adjoint_sweep(L, 1, A1, H, T1, s);
-    adjoint_sweep(L, 0, L.U, T1, T2, s);
-    // branch B: B2 = X(B1), B1 = Y(U)
-    adjoint_sweep(L, 0, B1, H, T1, s);
-    adjoint_sweep(L, 1, L.U, T1, T3, s);
-    adj::axpby_kernel<<<g2, b2, 0, s>>>(fld(T2, L), fld(T3, L), fld(L.lb_in, L), 1.0, 1.0, L.nx, L.ny);
+    sweep_transpose(L, 1, L.A1, L.flux[2], H, T1, nullptr, s);
+    sweep_transpose(L, 0, L.U, L.flux[0], T1, T2, nullptr, s);
+    // branch B: B2 = X(B1), B1 = Y(U); the sum of both branches is written at once
+    sweep_transpose(L, 0, L.B1, L.flux[3], H, T1, nullptr, s);
+    sweep_transpose(L, 1, L.U, L.flux[1], T1, L.lb_in, T2, s);
     return cudaGetLastError();
 }
 

@@ -121,8 +121,9 @@ struct fvm2d_solver {
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
     double *ckpt = nullptr;       // checkpoints of fvm2d_forward
-    double *seg = nullptr;        // states of one segment, recomputed by fvm2d_vjp
-    double *adj = nullptr;        // adjoint work: 2 adjoints + 13 work states + saved final state
+    double *tape = nullptr;       // one segment's steps, recomputed by fvm2d_vjp: per step its input
+                                  // state, X(U), Y(U) and the fluxes of its four sweeps
+    double *adj = nullptr;        // adjoint work: 2 adjoints, 3 work states, the saved final state
     int ck_count = 0, ck_len = 0, ck_cap = 0, seg_cap = 0, fwd_steps = -1;
     std::vector<double> ck_t;     // time at each checkpoint
     double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
@@ -323,7 +324,7 @@ int fvm2d_destroy(fvm2d_solver *s)
     if (s->ctl_h) cudaFreeHost(s->ctl_h);
     if (s->dual) cudaFree(s->dual);
     if (s->ckpt) cudaFree(s->ckpt);
-    if (s->seg) cudaFree(s->seg);
+    if (s->tape) cudaFree(s->tape);
     if (s->adj) cudaFree(s->adj);
     if (s->ev_begin) cudaEventDestroy(s->ev_begin);
     if (s->ev_end) cudaEventDestroy(s->ev_end);
@@ -684,16 +685,17 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
     const long long n4 = 4 * s->plane;
     const size_t sb = n4 * sizeof(double);
+    constexpr int kTapeStates = 7;  // per step: U, X(U), Y(U), the fluxes of its 4 sweeps
     if (s->ck_len > s->seg_cap) {
-        if (s->seg) cudaFree(s->seg);
-        s->seg = nullptr;
+        if (s->tape) cudaFree(s->tape);
+        s->tape = nullptr;
         s->seg_cap = 0;
-        CK(cudaMalloc(&s->seg, (size_t)s->ck_len * sb));
+        CK(cudaMalloc(&s->tape, (size_t)s->ck_len * kTapeStates * sb));
         s->seg_cap = s->ck_len;
     }
-    constexpr int kAdjStates = 16;  // two adjoints, 6 step work states, 7 sweep work states, the saved final state
+    constexpr int kAdjStates = 6;  // two adjoints, three work states, the saved final state
     if (!s->adj) CK(cudaMalloc(&s->adj, kAdjStates * sb));
-    double *lam = s->adj, *lam2 = s->adj + n4, *saved = s->adj + 15 * n4;
+    double *lam = s->adj, *lam2 = s->adj + n4, *saved = s->adj + 5 * n4;
     fvm2d::AdjointLaunch L;
     L.nx = s->nx;
     L.ny = s->ny;
@@ -708,15 +710,15 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     L.alpha = s->alpha;
     L.gamma = s->gamma;
     L.dt = s->fixed_dt;
-    for (int k = 0; k < 6; ++k) L.state[k] = s->adj + (2 + k) * n4;
-    for (int k = 0; k < 7; ++k) L.work[k] = s->adj + (8 + k) * n4;
+    for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * n4;
     const StepControl after = *s->ctl_h;
     CK(cudaMemcpyAsync(saved, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
     if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
     StepControl *h = s->ctl_h;
+    auto tape = [&](int j, int q) { return s->tape + ((long long)j * kTapeStates + q) * n4; };
     for (int k = s->ck_count - 1; k >= 0; --k) {
         const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
-        // recompute the segment from its checkpoint, keeping the input of every step
+        // recompute the segment from its checkpoint, taping every step
         CK(cudaMemcpyAsync(s->U, s->ckpt + k * n4, sb, cudaMemcpyDeviceToDevice, s->stream));
         std::memset(h, 0, sizeof(StepControl));
         h->t = s->ck_t[k];
@@ -724,12 +726,19 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
         if (int rc = s->upload_control()) return rc;
         CK(kVariants[FVM2D_FP64].plan(c, s->stream));
         for (int j = 0; j < m; ++j) {
-            CK(cudaMemcpyAsync(s->seg + j * n4, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-            if (j + 1 < m) CK(kVariants[FVM2D_FP64].step(c, s->stream, nullptr));
+            CK(cudaMemcpyAsync(tape(j, 0), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+            LaunchConfig cj = c;
+            cj.A = tape(j, 1);
+            cj.B = tape(j, 2);
+            void *const flux[4] = {tape(j, 3), tape(j, 4), tape(j, 5), tape(j, 6)};
+            CK(fvm2d::fp64::enqueue_step_taped(cj, s->stream, flux));
         }
         // reverse through the segment
         for (int j = m - 1; j >= 0; --j) {
-            L.U = s->seg + j * n4;
+            L.U = tape(j, 0);
+            L.A1 = tape(j, 1);
+            L.B1 = tape(j, 2);
+            for (int q = 0; q < 4; ++q) L.flux[q] = tape(j, 3 + q);
             L.lb_out = lam;
             L.lb_in = lam2;
             CK(fvm2d::adjoint_step(L, s->stream));

@@ -4,6 +4,7 @@
 #define FVM2D_VARIANT fp64
 #define FVM2D_REAL double
 #define FVM2D_PHYS Hoisted
+#define FVM2D_TAPED_STEP  // also the taped step of the differentiation form
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to; measured best for this build at 4096^2
 #ifdef FVM2D_TUNE_X

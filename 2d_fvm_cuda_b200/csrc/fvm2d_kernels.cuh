@@ -125,6 +125,8 @@ struct SweepArgs {
     double rh;         // 1.0 / h, as the reference computes it
     double alpha, gamma;
     StepControl *ctl;
+    Field<Real> flux;  // taped sweeps only: each interface's flux (planes: mass, normal
+                       // momentum, energy, tangential momentum) at the interface's right cell
 };
 
 // Wave speed of all cells of the initial state, then the first step's plan.
@@ -237,8 +239,9 @@ __device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
 constexpr int kXCells = 30;
 
 // One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
-// wave speed of the interior cells written by a final sweep.
-template <typename Real, class Phys, bool FINAL>
+// wave speed of the interior cells written by a final sweep; a TAPE sweep
+// also stores every interface flux it computes.
+template <typename Real, class Phys, bool FINAL, bool TAPE = false>
 __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int y, int seg,
                                        int nseg, int lane, double &vmax)
 {
@@ -253,6 +256,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
     const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
     Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
     if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+    if (TAPE && lane >= 1 && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // interface c-1/2 at cell c
     const Cell<Real> FR = shfl_down(F);
     auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
         if (FINAL) {
@@ -283,7 +287,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
     }
 }
 
-template <typename Real, class Phys, bool FINAL, int NT, int MINB>
+template <typename Real, class Phys, bool FINAL, int NT, int MINB, bool TAPE = false>
 __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
 {
     if (!a.ctl->active) return;
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
     for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
-        x_item<Real, Phys, FINAL>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax);
+        x_item<Real, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax);
     if (FINAL) block_max_to<NT>(vmax, &a.ctl->smax_bits);
 }
 
@@ -302,8 +306,8 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
 __host__ __device__ __forceinline__ int y_segments(int ny, int T) { return (ny - 4 + T - 2) / (T - 1); }
 
 // One y-sweep work item: columns 32 cw .. 32 cw + 31, segment seg (of nseg)
-// of T interfaces.
-template <typename Real, class Phys>
+// of T interfaces.  A TAPE sweep also stores every interface flux.
+template <typename Real, class Phys, bool TAPE = false>
 __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int seg, int nseg,
                                        int cw, int lane, int T)
 {
@@ -321,6 +325,7 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
         const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
         const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
         const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+        if (TAPE && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);  // interface l-1/2 at line position l
         if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
         Fp = F;
         cm1 = c0;
@@ -335,7 +340,7 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
         for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
 }
 
-template <typename Real, class Phys, int NT, int MINB>
+template <typename Real, class Phys, int NT, int MINB, bool TAPE = false>
 __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, int T)
 {
     if (!a.ctl->active) return;
@@ -346,7 +351,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, in
     const long long nwork = (long long)ncw * nseg;
     const long long wstride = (long long)gridDim.x * (NT / 32);
     for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
-        y_item<Real, Phys>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T);
+        y_item<Real, Phys, TAPE>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T);
 }
 
 // ---------------------------------------------------------------------------
