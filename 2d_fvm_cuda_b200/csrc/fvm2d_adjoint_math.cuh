@@ -612,9 +612,9 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
         rho_rb += a_r * Dr;
         a_rb += rho_r * Dr;
     }
-    // a = sqrt(g pi irho)
+    // a = sqrt(g pi irho); 1/a = rho il
     {
-        const A al = a_lb / (two * a_l), ar = a_rb / (two * a_r);
+        const A al = half * a_lb * rho_l * il, ar = half * a_rb * rho_r * ir;
         pi_lb += g * irl * al;
         irlb += g * pi_l * al;
         pi_rb += g * irr * ar;

@@ -648,6 +648,7 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
         CK(cudaMalloc(&s->ckpt, (size_t)count * n4 * sizeof(double)));
         s->ck_cap = count;
     }
+    if (int rc = s->build_graphs()) return rc;  // the step graphs of the fixed-dt FP64 build
     StepControl *h = s->ctl_h;
     h->step_limit = INT_MAX;
     h->done = 0;
@@ -662,9 +663,11 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
         s->ck_t[k] = t;
         CK(cudaMemcpyAsync(s->ckpt + k * n4, s->U, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         const int m = (k + 1) * len <= nsteps ? len : nsteps - k * len;
-        for (int j = 0; j < m; ++j) {
-            CK(kVariants[FVM2D_FP64].step(c, s->stream, nullptr));
-            t = t + s->fixed_dt;  // the same addition the device does
+        for (int j = 0; j < m;) {
+            const int which = m - j >= fvm2d_solver::kGraphSteps[0] ? 0 : 1;
+            CK(cudaGraphLaunch(s->graph[which], s->stream));
+            for (int q = 0; q < fvm2d_solver::kGraphSteps[which]; ++q) t = t + s->fixed_dt;  // as the device adds
+            j += fvm2d_solver::kGraphSteps[which];
         }
     }
     CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
