@@ -329,17 +329,22 @@ void sweep_transpose(const AdjointLaunch &L, int dir, const double *U, const dou
 
 } // namespace
 
+cudaError_t adjoint_prepare()
+{
+    if (g_sms) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_x, adj::adjoint_x_kernel, adj::ANT, 0))) return e;
+    if (g_occ_x < 1) g_occ_x = 1;
+    g_sms = sms;
+    return cudaSuccess;
+}
+
 cudaError_t adjoint_step(const AdjointLaunch &L, cudaStream_t s)
 {
-    if (!g_sms) {
-        int dev = 0;
-        cudaError_t e;
-        if ((e = cudaGetDevice(&dev))) return e;
-        if ((e = cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev))) return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_x, adj::adjoint_x_kernel, adj::ANT, 0)))
-            return e;
-        if (g_occ_x < 1) g_occ_x = 1;
-    }
+    if (cudaError_t e = adjoint_prepare()) return e;
     double *H = L.work[0], *T1 = L.work[1], *T2 = L.work[2];
     // ghost fill and average, transposed: H = ghost^T(lb_out) / 2
     const dim3 g2((L.nx + 31) / 32, (L.ny + 7) / 8), b2(32, 8);

@@ -20,6 +20,10 @@ struct AdjointLaunch {
     double *work[3];        // work states
 };
 
+// Queries the device once (SM count, occupancy); call before capturing
+// adjoint steps into a graph.  adjoint_step calls it too.
+cudaError_t adjoint_prepare();
+
 cudaError_t adjoint_step(const AdjointLaunch &L, cudaStream_t s);
 
 } // namespace fvm2d

@@ -125,6 +125,10 @@ struct fvm2d_solver {
                                   // state, X(U), Y(U) and the fluxes of its four sweeps
     double *adj = nullptr;        // adjoint work: 2 adjoints, 3 work states, the saved final state
     int ck_count = 0, ck_len = 0, ck_cap = 0, seg_cap = 0, fwd_steps = -1;
+    // fvm2d_vjp's graphs for a full segment: its taped recompute, and its
+    // reverse starting from either adjoint buffer; built for vjp_len steps
+    cudaGraphExec_t vjp_graph[3] = {nullptr, nullptr, nullptr};
+    int vjp_len = 0;
     std::vector<double> ck_t;     // time at each checkpoint
     double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
     double last_device_ms = 0.0;  // CUDA-event time of the last loop on the stream
@@ -164,6 +168,38 @@ struct fvm2d_solver {
             g = nullptr;
         }
         graph_variant = -1;
+        drop_vjp_graphs();
+    }
+
+    void drop_vjp_graphs()
+    {
+        for (auto &g : vjp_graph) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+        vjp_len = 0;
+    }
+
+    // Captures what `enqueue` puts on the stream into *out.
+    template <class F>
+    int capture(cudaGraphExec_t *out, F &&enqueue)
+    {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue();
+        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+        cudaError_t e = cudaGraphInstantiate(out, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            *out = nullptr;
+            return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        return FVM2D_OK;
     }
 
     int build_graphs()
@@ -690,6 +726,7 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     const size_t sb = n4 * sizeof(double);
     constexpr int kTapeStates = 7;  // per step: U, X(U), Y(U), the fluxes of its 4 sweeps
     if (s->ck_len > s->seg_cap) {
+        s->drop_vjp_graphs();
         if (s->tape) cudaFree(s->tape);
         s->tape = nullptr;
         s->seg_cap = 0;
@@ -697,7 +734,10 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
         s->seg_cap = s->ck_len;
     }
     constexpr int kAdjStates = 6;  // two adjoints, three work states, the saved final state
-    if (!s->adj) CK(cudaMalloc(&s->adj, kAdjStates * sb));
+    if (!s->adj) {
+        s->drop_vjp_graphs();
+        CK(cudaMalloc(&s->adj, kAdjStates * sb));
+    }
     double *lam = s->adj, *lam2 = s->adj + n4, *saved = s->adj + 5 * n4;
     fvm2d::AdjointLaunch L;
     L.nx = s->nx;
@@ -719,6 +759,45 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
     StepControl *h = s->ctl_h;
     auto tape = [&](int j, int q) { return s->tape + ((long long)j * kTapeStates + q) * n4; };
+    // the taped recompute of m steps from the state in U, and the reverse of
+    // m steps from adjoint buffer `from` (the result lands in `from` for even m)
+    auto recompute = [&](int m) -> int {
+        for (int j = 0; j < m; ++j) {
+            CK(cudaMemcpyAsync(tape(j, 0), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+            LaunchConfig cj = c;
+            cj.A = tape(j, 1);
+            cj.B = tape(j, 2);
+            void *const flux[4] = {tape(j, 3), tape(j, 4), tape(j, 5), tape(j, 6)};
+            CK(fvm2d::fp64::enqueue_step_taped(cj, s->stream, flux));
+        }
+        return FVM2D_OK;
+    };
+    double *const adj0 = s->adj, *const adj1 = s->adj + n4;
+    auto reverse = [&](int m, double *from) -> int {
+        double *a = from, *b = from == adj0 ? adj1 : adj0;
+        for (int j = m - 1; j >= 0; --j) {
+            L.U = tape(j, 0);
+            L.A1 = tape(j, 1);
+            L.B1 = tape(j, 2);
+            for (int q = 0; q < 4; ++q) L.flux[q] = tape(j, 3 + q);
+            L.lb_out = a;
+            L.lb_in = b;
+            CK(fvm2d::adjoint_step(L, s->stream));
+            std::swap(a, b);
+        }
+        return FVM2D_OK;
+    };
+    // graphs of a full segment, kept while the handle's parameters and
+    // buffers stay the same
+    if (s->vjp_len != s->ck_len && s->ck_count > 1) {
+        s->drop_vjp_graphs();
+        CK(fvm2d::adjoint_prepare());
+        const int len = s->ck_len;
+        if (int rc = s->capture(&s->vjp_graph[0], [&] { return recompute(len); })) return rc;
+        if (int rc = s->capture(&s->vjp_graph[1], [&] { return reverse(len, adj0); })) return rc;
+        if (int rc = s->capture(&s->vjp_graph[2], [&] { return reverse(len, adj1); })) return rc;
+        s->vjp_len = len;
+    }
     for (int k = s->ck_count - 1; k >= 0; --k) {
         const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
         // recompute the segment from its checkpoint, taping every step
@@ -728,25 +807,15 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
         h->step_limit = INT_MAX;
         if (int rc = s->upload_control()) return rc;
         CK(kVariants[FVM2D_FP64].plan(c, s->stream));
-        for (int j = 0; j < m; ++j) {
-            CK(cudaMemcpyAsync(tape(j, 0), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-            LaunchConfig cj = c;
-            cj.A = tape(j, 1);
-            cj.B = tape(j, 2);
-            void *const flux[4] = {tape(j, 3), tape(j, 4), tape(j, 5), tape(j, 6)};
-            CK(fvm2d::fp64::enqueue_step_taped(cj, s->stream, flux));
+        const bool full = m == s->vjp_len;
+        if (full) {
+            CK(cudaGraphLaunch(s->vjp_graph[0], s->stream));
+            CK(cudaGraphLaunch(s->vjp_graph[lam == adj0 ? 1 : 2], s->stream));
+        } else {
+            if (int rc = recompute(m)) return rc;
+            if (int rc = reverse(m, lam)) return rc;
         }
-        // reverse through the segment
-        for (int j = m - 1; j >= 0; --j) {
-            L.U = tape(j, 0);
-            L.A1 = tape(j, 1);
-            L.B1 = tape(j, 2);
-            for (int q = 0; q < 4; ++q) L.flux[q] = tape(j, 3 + q);
-            L.lb_out = lam;
-            L.lb_in = lam2;
-            CK(fvm2d::adjoint_step(L, s->stream));
-            std::swap(lam, lam2);
-        }
+        if (m & 1) std::swap(lam, lam2);
     }
     if (int rc = planes_to_cells(s, lam, cotangent_out, stride)) return rc;
     CK(cudaMemcpyAsync(s->U, saved, sb, cudaMemcpyDeviceToDevice, s->stream));
