@@ -8,9 +8,10 @@ The package directory name starts with a digit, so import it with
 * ``Handle`` -- one C-ABI solver handle (include/fvm2d.h), for callers that
   want the state to stay on the GPU between calls.
 * ``Batch`` -- many independent problems of different sizes solved together.
+* ``slab`` -- one problem split by rows across processes (one GPU each).
 * ``scenarios`` -- initial data (the reference's demo problems and seeded
   workloads).
 """
-from . import scenarios  # noqa: F401
+from . import scenarios, slab  # noqa: F401
 from ._lib import FP32, FP64, FP64_REFORDER, FP64_STRICT, Batch, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
 from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

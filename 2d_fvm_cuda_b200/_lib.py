@@ -39,6 +39,11 @@ SIGNATURES = [
     ("fvm2d_get_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     ("fvm2d_solve", ctypes.c_int, [_vp]),
     ("fvm2d_advance", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_advance_dt", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_get_wave_speed_max", ctypes.c_int, [_vp, _dp]),
+    ("fvm2d_set_row_frame", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("fvm2d_get_rows", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    ("fvm2d_set_rows", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
     ("fvm2d_get_computation_time_ms", ctypes.c_int, [_vp, _dp]),
     ("fvm2d_get_time_stages_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
@@ -193,6 +198,41 @@ class Handle:
         k = ctypes.c_int(0)
         check(self.lib.fvm2d_profile_kernels(self.h, int(nsteps), out, ctypes.byref(k)))
         return list(out), k.value
+
+    # -- row slabs (one problem split across processes) --
+    def advance_dt(self, dt: float) -> None:
+        """One step with the caller's dt."""
+        check(self.lib.fvm2d_advance_dt(self.h, float(dt)))
+
+    def wave_speed_max(self) -> float:
+        v = ctypes.c_double(0)
+        check(self.lib.fvm2d_get_wave_speed_max(self.h, ctypes.byref(v)))
+        return v.value
+
+    def set_row_frame(self, row0: int, ny_global: int, fill_top: bool, fill_bottom: bool) -> None:
+        check(self.lib.fvm2d_set_row_frame(self.h, int(row0), int(ny_global), int(bool(fill_top)),
+                                           int(bool(fill_bottom))))
+
+    def get_rows(self, j0: int, nrows: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Rows j0 .. j0+nrows-1 as a (4, nrows, nx) array (planes rho, p, u, v)."""
+        if out is None:
+            out = np.empty((4, nrows, self.nx))
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == 4 * nrows * self.nx
+        check(self.lib.fvm2d_get_rows(self.h, int(j0), int(nrows), out.ctypes.data))
+        return out
+
+    def set_rows(self, j0: int, rows: np.ndarray) -> None:
+        R = np.ascontiguousarray(rows, dtype=np.float64)
+        nrows = R.size // (4 * self.nx)
+        assert R.size == 4 * nrows * self.nx
+        check(self.lib.fvm2d_set_rows(self.h, int(j0), int(nrows), R.ctypes.data))
+
+    def get_rows_ptr(self, j0: int, nrows: int, ptr: int) -> None:
+        """As get_rows, into host or device memory at ptr (4*nrows*nx doubles)."""
+        check(self.lib.fvm2d_get_rows(self.h, int(j0), int(nrows), ptr))
+
+    def set_rows_ptr(self, j0: int, nrows: int, ptr: int) -> None:
+        check(self.lib.fvm2d_set_rows(self.h, int(j0), int(nrows), ptr))
 
     # -- differentiation (fixed dt, FP64 build) --
     def set_fixed_dt(self, dt: float) -> None:

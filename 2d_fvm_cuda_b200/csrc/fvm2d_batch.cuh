@@ -177,6 +177,9 @@ __global__ void __launch_bounds__(NT) batch_ghost_kernel(BatchArgs<Real> b)
     g.gamma = P.gamma;
     g.ctl = ctl;
     g.plan = P.plan;
+    g.row0 = 0;
+    g.gny = P.ny;
+    g.fill_top = g.fill_bottom = 1;
     const double t = ctl->t + ctl->dt;
     const int k = (int(blockIdx.x) - b.rb0[p]) * NT + threadIdx.x;
     const double v = (k < P.ring) ? ghost_cell(g, k, t) : 0.0;

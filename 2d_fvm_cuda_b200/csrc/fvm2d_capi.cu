@@ -30,6 +30,8 @@ using fvm2d::StepControl;
 using fvm2d::aos_to_soa;
 using fvm2d::convert_planes;
 using fvm2d::is_device_pointer;
+using fvm2d::rows_in;
+using fvm2d::rows_out;
 using fvm2d::soa_to_aos;
 
 namespace {
@@ -118,6 +120,7 @@ struct fvm2d_solver {
     bool have_state = false;
     bool need_init = true;
     double fixed_dt = 0.0;        // > 0: differentiation runs step with this constant dt
+    int row0 = 0, ny_global = 0, fill_top = 1, fill_bottom = 1;  // row frame of a slab (fvm2d_set_row_frame)
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
     double *ckpt = nullptr;       // checkpoints of fvm2d_forward
@@ -148,7 +151,7 @@ struct fvm2d_solver {
         c.B = scratch + 4 * plane;
         c.ctl = ctl;
         c.hx = width / double(nx);
-        c.hy = height / double(ny);
+        c.hy = height / double(ny_global > 0 ? ny_global : ny);  // a slab keeps the problem's row spacing
         c.rhx = 1.0 / c.hx;
         c.rhy = 1.0 / c.hy;
         c.alpha = alpha;
@@ -158,6 +161,10 @@ struct fvm2d_solver {
         c.plan.cfl = cfl;
         c.plan.hmin = (c.hy < c.hx) ? c.hy : c.hx;
         c.plan.fixed_dt = fixed_dt;
+        c.row0 = row0;
+        c.ny_global = ny_global;
+        c.fill_top = fill_top;
+        c.fill_bottom = fill_bottom;
         return c;
     }
 
@@ -512,6 +519,107 @@ int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done)
     if (int rc = s->loop(1, nsteps)) return rc;
     s->total_steps += c->steps - before;
     if (steps_done) *steps_done = c->steps - before;
+    return FVM2D_OK;
+}
+
+int fvm2d_advance_dt(fvm2d_solver *s, double dt)
+{
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(FVM2D_ERR_INVALID, "dt must be positive and finite");
+    const LaunchConfig cfg = s->config();
+    if (int rc = s->build_graphs()) return rc;
+    StepControl *c = s->ctl_h;
+    if (s->need_init) {  // wave-speed max of the fresh state; the device record becomes the reference
+        CK(kVariants[s->precision].init(cfg, s->stream));
+        s->need_init = false;
+        CK(cudaMemcpyAsync(c, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    c->dt = dt;
+    c->active = 1;
+    c->done = 0;
+    c->step_limit = c->steps + 1;
+    if (int rc = s->upload_control()) return rc;
+    CK(cudaEventRecord(s->ev_begin, s->stream));
+    CK(cudaGraphLaunch(s->graph[1], s->stream));
+    CK(cudaMemcpyAsync(c, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaEventRecord(s->ev_end, s->stream));
+    CK(cudaEventSynchronize(s->ev_end));
+    float dms = 0.f;
+    CK(cudaEventElapsedTime(&dms, s->ev_begin, s->ev_end));
+    s->last_device_ms = dms;
+    s->last_launches = fvm2d::kStepKernels;
+    s->total_steps += 1;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_wave_speed_max(fvm2d_solver *s, double *smax)
+{
+    if (int rc = check(s)) return rc;
+    if (!smax) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (s->need_init) {
+        CK(kVariants[s->precision].init(s->config(), s->stream));
+        s->need_init = false;
+        CK(cudaMemcpyAsync(s->ctl_h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    *smax = s->ctl_h->smax_last;
+    return FVM2D_OK;
+}
+
+int fvm2d_set_row_frame(fvm2d_solver *s, int row0, int ny_global, int fill_top, int fill_bottom)
+{
+    if (int rc = check(s)) return rc;
+    if (ny_global == 0) {
+        row0 = 0;
+        fill_top = fill_bottom = 1;
+    } else if (row0 < 0 || ny_global < row0 + s->ny) {
+        return fail(FVM2D_ERR_INVALID, "the slab must lie inside the global rows: 0 <= row0, row0 + ny <= ny_global");
+    }
+    s->row0 = row0;
+    s->ny_global = ny_global;
+    s->fill_top = fill_top ? 1 : 0;
+    s->fill_bottom = fill_bottom ? 1 : 0;
+    s->drop_graph();
+    return FVM2D_OK;
+}
+
+static int rows_check(fvm2d_solver *s, int j0, int nrows, const void *buf)
+{
+    if (int rc = check(s)) return rc;
+    if (!buf) return fail(FVM2D_ERR_INVALID, "null row buffer");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (j0 < 0 || nrows < 1 || j0 + nrows > s->ny) return fail(FVM2D_ERR_INVALID, "rows out of range");
+    return FVM2D_OK;
+}
+
+int fvm2d_get_rows(fvm2d_solver *s, int j0, int nrows, double *rows)
+{
+    if (int rc = rows_check(s, j0, nrows, rows)) return rc;
+    if (is_fp32(s->precision))
+        rows_out<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->plane, s->pitch, j0,
+                                                        nrows, s->nx, s->scratch);
+    else
+        rows_out<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rows, s->scratch, sizeof(double) * 4 * (size_t)nrows * s->nx, cudaMemcpyDefault, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FVM2D_OK;
+}
+
+int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows)
+{
+    if (int rc = rows_check(s, j0, nrows, rows)) return rc;
+    CK(cudaMemcpyAsync(s->scratch, rows, sizeof(double) * 4 * (size_t)nrows * s->nx, cudaMemcpyDefault, s->stream));
+    if (is_fp32(s->precision))
+        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, j0, nrows,
+                                                       s->nx, s->scratch);
+    else
+        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
     return FVM2D_OK;
 }
 

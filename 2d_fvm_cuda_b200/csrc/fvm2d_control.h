@@ -39,6 +39,12 @@ struct LaunchConfig {
     double alpha, gamma;
     int strategy;
     PlanParams plan;
+    // Row frame when the array is one row slab of a larger one (a problem
+    // split across processes): the global row of local row 0, the global row
+    // count (0: ny), and whether the preset fills the top ghost rows (0, 1)
+    // and the bottom ones.  Ring rows it does not fill are halo rows, left out
+    // of the wave-speed max.
+    int row0 = 0, ny_global = 0, fill_top = 1, fill_bottom = 1;
 };
 
 // Kernels per step: sweep X, sweep Y, sweep Y, sweep X + average, ghost ring.

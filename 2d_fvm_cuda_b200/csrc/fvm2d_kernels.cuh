@@ -377,6 +377,8 @@ struct GhostArgs {
     double gamma;
     StepControl *ctl;
     PlanParams plan;
+    int row0, gny;               // global row of local row 0; global row count
+    int fill_top, fill_bottom;   // 0: that pair of ring rows is a halo (not filled, no max)
 };
 
 template <typename Real>
@@ -415,8 +417,8 @@ __device__ __forceinline__ Cell<Real> row_rule(const GhostArgs<Real> &a, int i, 
         return c;
     default: {  // REFLECTIVE, DOUBLE_MACH: ghostCellPresets.cuh:56-92
         if (j == 0 || j == 1) {
-            double temp = double(ny) / sqrt(3.0);
-            double dist = double(ny) * 20 * t / sqrt(3.0);
+            double temp = double(a.gny) / sqrt(3.0);
+            double dist = double(a.gny) * 20 * t / sqrt(3.0);
             if (i <= nx / 24 + int(temp) + int(dist)) return mk<Real>(8, 116.5, 4.125 * sqrt(3.0), -4.125);
             return mk<Real>(1.4, 1, 0, 0);
         }
@@ -455,13 +457,14 @@ __device__ __forceinline__ Cell<Real> col_rule(const GhostArgs<Real> &a, int i, 
         return after_rows(a, left ? 2 : nx - 3, j, t);
     case JET:  // ghostCellPresets.cuh:173-191
         if (left) {
-            if (j >= 2 * ny / 5 + 1 && j <= 3 * ny / 5) return mk<Real>(5.0, 0.4127, 800.0, 0.0);
+            const int gj = a.row0 + j, gny = a.gny;
+            if (gj >= 2 * gny / 5 + 1 && gj <= 3 * gny / 5) return mk<Real>(5.0, 0.4127, 800.0, 0.0);
             return mk<Real>(0.5, 0.4127, 0.0, 0.0);
         }
         return after_rows(a, nx - 3, j, t);
     case JET800:  // ghostCellPresets.cuh:221-239
         if (left) {
-            if (j >= 9 * ny / 10) return mk<Real>(1.4, 1, 800, 0);
+            if (a.row0 + j >= 9 * a.gny / 10) return mk<Real>(1.4, 1, 800, 0);
             return mk<Real>(0.14, 1, 0, 0);
         }
         return after_rows(a, nx - 3, j, t);
@@ -484,6 +487,7 @@ __device__ __forceinline__ double ghost_cell(const GhostArgs<Real> &a, int k, do
     int i, j;
     if (k < nrow) {
         const int r = k / nx;
+        if (!(r < 2 ? a.fill_top : a.fill_bottom)) return 0.0;  // halo rows of a slab
         i = k % nx;
         j = r < 2 ? r : ny - 4 + r;
     } else {

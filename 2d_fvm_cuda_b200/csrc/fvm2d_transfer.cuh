@@ -40,6 +40,30 @@ static __global__ void convert_planes(const S *__restrict__ in, D *__restrict__ 
         out[k] = D(in[k]);
 }
 
+// Rows j0 .. j0+nrows-1 of the four planes, packed as [4][nrows][nx] doubles
+// (rows_out) and back (rows_in).
+template <typename T>
+static __global__ void rows_out(const T *__restrict__ U, long long plane, int pitch, int j0, int nrows, int nx,
+                                double *__restrict__ out)
+{
+    const long long per = (long long)nrows * nx, n = 4 * per;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int f = int(k / per), r = int(k % per / nx), x = int(k % nx);
+        out[k] = double(U[f * plane + (long long)(j0 + r) * pitch + x]);
+    }
+}
+
+template <typename T>
+static __global__ void rows_in(T *__restrict__ U, long long plane, int pitch, int j0, int nrows, int nx,
+                               const double *__restrict__ in)
+{
+    const long long per = (long long)nrows * nx, n = 4 * per;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int f = int(k / per), r = int(k % per / nx), x = int(k % nx);
+        U[f * plane + (long long)(j0 + r) * pitch + x] = T(in[k]);
+    }
+}
+
 inline bool is_device_pointer(const void *p)
 {
     cudaPointerAttributes a;

@@ -137,6 +137,34 @@ int fvm2d_solve(fvm2d_solver *s);
  * benchmarks). */
 int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done);
 
+/* ---- row slabs (no reference counterpart) ---------------------------------
+ * One problem split by rows across processes (2d_fvm_cuda_b200/slab.py): each
+ * process holds a slab with two halo rows per inner edge, exchanges them
+ * between steps and steps with a dt agreed across processes. */
+
+/* One step with the caller's dt (the CFL rule applied by the caller, e.g.
+ * over all slabs).  The ghost fill and time advance are as in fvm2d_advance. */
+int fvm2d_advance_dt(fvm2d_solver *s, double dt);
+
+/* Max over the cells of the current state of |(u, v)| + sqrt(gamma p / rho),
+ * the quantity of the reference's CFL rule (src/basicFuns.cuh:215-226,
+ * src/wrappers.cuh:198-202); halo rows of a slab are left out after a step. */
+int fvm2d_get_wave_speed_max(fvm2d_solver *s, double *smax);
+
+/* The array is rows row0 .. row0+ny-1 of a problem of ny_global rows whose
+ * height is the spatial layout's: the row spacing is height / ny_global, the
+ * presets see global row numbers, and they fill the top ghost rows (0, 1)
+ * only if fill_top and the bottom ones only if fill_bottom.  Ring rows they do
+ * not fill are halo rows, left out of the wave-speed max (their values are
+ * the caller's to replace before the next step).  ny_global = 0 restores a
+ * whole problem. */
+int fvm2d_set_row_frame(fvm2d_solver *s, int row0, int ny_global, int fill_top, int fill_bottom);
+
+/* Rows j0 .. j0+nrows-1 of the state as [4][nrows][nx] doubles (planes rho,
+ * p, u, v), from or into host or device memory. */
+int fvm2d_get_rows(fvm2d_solver *s, int j0, int nrows, double *rows);
+int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows);
+
 /* getComputationTime_ms (src/wrappers.cuh:308-311): wall time of the last
  * solve()/advance() loop in milliseconds. */
 int fvm2d_get_computation_time_ms(fvm2d_solver *s, double *ms);
