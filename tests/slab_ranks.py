@@ -90,7 +90,7 @@ def _init(rank, world, port):
     return dist
 
 
-def cpu_worker(rank, world, port, case, out_q):
+def cpu_worker(rank, world, port, case, out_path):
     dist = _init(rank, world, port)
     try:
         pkg = importlib.import_module("2d_fvm_cuda_b200")
@@ -103,13 +103,13 @@ def cpu_worker(rank, world, port, case, out_q):
                                 make_local=lambda nx, rows: OracleSlab(orc, nx, rows))
         S.advance(case["steps"])
         G = S.gather()
-        if rank == 0:
-            out_q.put((G, S.t, S.steps))
+        if rank == 0:  # through a file: a pipe would block on results above its 64 KB buffer
+            np.savez(out_path, G=G, t=S.t, steps=S.steps)
     finally:
         dist.destroy_process_group()
 
 
-def gpu_worker(rank, world, port, case, out_q):
+def gpu_worker(rank, world, port, case, out_path):
     """A rank with the real GPU solver (libfvm2d); ranks share one GPU and
     exchange rows through host memory (gloo).  No kernel waits on another
     rank: the exchange happens between steps, on the host."""
@@ -122,7 +122,7 @@ def gpu_worker(rank, world, port, case, out_q):
         S.solve()
         G = S.gather()
         S.close()
-        if rank == 0:
-            out_q.put((G, S.t, S.steps))
+        if rank == 0:  # through a file: a pipe would block on results above its 64 KB buffer
+            np.savez(out_path, G=G, t=S.t, steps=S.steps)
     finally:
         dist.destroy_process_group()

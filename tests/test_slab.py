@@ -50,18 +50,18 @@ def test_halo_messages_fill_every_halo_row(pkg):
 
 
 CASES = [
-    dict(world=2, nx=36, ny=41, seed=3, strategy=0, width=1.0, height=1.1, t_end=0.05, steps=12),
+    dict(world=2, nx=64, ny=57, seed=3, strategy=0, width=1.0, height=1.1, t_end=0.05, steps=12),
     dict(world=3, nx=33, ny=46, seed=4, strategy=5, width=1.0, height=1.0, t_end=0.05, steps=12),
     dict(world=2, nx=40, ny=30, seed=5, strategy=6, width=1.2, height=1.0, t_end=0.05, steps=12),
 ]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"world{c['world']}-strategy{c['strategy']}")
-def test_slab_run_equals_single_array_run(oracle, case):
-    ctx = mp.get_context("spawn")
-    q = ctx.SimpleQueue()
-    mp.spawn(slab_ranks.cpu_worker, args=(case["world"], free_port(), case, q), nprocs=case["world"], join=True)
-    G, t, steps = q.get()
+def test_slab_run_equals_single_array_run(oracle, case, tmp_path):
+    out = str(tmp_path / "gathered.npz")
+    mp.spawn(slab_ranks.cpu_worker, args=(case["world"], free_port(), case, out), nprocs=case["world"], join=True)
+    z = np.load(out)
+    G, t, steps = z["G"], float(z["t"]), int(z["steps"])
     U = slab_ranks.initial_state(case["nx"], case["ny"], case["seed"], case["strategy"])
     R, rsteps, rt = oracle.solve(U, max_steps=case["steps"], width=case["width"], height=case["height"], cfl=0.45,
                                  alpha=1.9, gamma=1.4, t_end=case["t_end"], strategy=case["strategy"])
