@@ -210,51 +210,29 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
         }
     }
     // ---- reverse: midpoint flux ----
-    Cell5 Wb = {0, 0, 0, 0, 0}, Wtb = {0, 0, 0, 0, 0};
+    // F.rho = m + hk mt; F.p = m un + p + hk (mt un + m un_t + p_t);
+    // F.un (energy) = m es + p un + hk (mt es + m q + p_t un + p un_t);
+    // F.ut = m ut + hk (mt ut + m ut_t), with m = rho un, mt = rho un_t + un rho_t,
+    // es = e + (un^2 + ut^2)/2, q = e_t + un un_t + ut ut_t
+    Cell5 Wb, Wtb;
     {
         const A m = W.rho * W.un, mt = W.rho * Wt.un + W.un * Wt.rho;
         const A es = W.e + half * (W.un * W.un + W.ut * W.ut);
         const A q = Wt.e + W.un * Wt.un + W.ut * Wt.ut;
-        A mb = 0, mtb = 0, esb = 0, qb = 0;
-        // F.ut = m ut + hk (mt ut + m ut_t)
-        mb += (W.ut + hk * Wt.ut) * Fb.ut;
-        Wb.ut += (m + hk * mt) * Fb.ut;
-        mtb += hk * W.ut * Fb.ut;
-        Wtb.ut += hk * m * Fb.ut;
-        // F.un (energy) = m es + p un + hk (mt es + m q + p_t un + p un_t)
-        mb += (es + hk * q) * Fb.un;
-        esb += (m + hk * mt) * Fb.un;
-        Wb.p += (W.un + hk * Wt.un) * Fb.un;
-        Wb.un += (W.p + hk * Wt.p) * Fb.un;
-        mtb += hk * es * Fb.un;
-        qb += hk * m * Fb.un;
-        Wtb.p += hk * W.un * Fb.un;
-        Wtb.un += hk * W.p * Fb.un;
-        // q = e_t + un un_t + ut ut_t
-        Wtb.e += qb;
-        Wb.un += Wt.un * qb;
-        Wtb.un += W.un * qb;
-        Wb.ut += Wt.ut * qb;
-        Wtb.ut += W.ut * qb;
-        // F.p (normal momentum) = m un + p + hk (mt un + m un_t + p_t)
-        mb += (W.un + hk * Wt.un) * Fb.p;
-        Wb.un += (m + hk * mt) * Fb.p;
-        Wb.p += Fb.p;
-        mtb += hk * W.un * Fb.p;
-        Wtb.un += hk * m * Fb.p;
-        Wtb.p += hk * Fb.p;
-        // F.rho (mass) = m + hk mt
-        mb += Fb.rho;
-        mtb += hk * Fb.rho;
-        // es = e + (un^2 + ut^2)/2
-        Wb.e += esb;
-        Wb.un += W.un * esb;
-        Wb.ut += W.ut * esb;
-        // mt = rho un_t + un rho_t ; m = rho un
-        Wb.rho += Wt.un * mtb + W.un * mb;
-        Wtb.un += W.rho * mtb;
-        Wb.un += Wt.rho * mtb + W.rho * mb;
-        Wtb.rho += W.un * mtb;
+        const A hr = hk * Fb.rho, hp = hk * Fb.p, he = hk * Fb.un, hu = hk * Fb.ut;
+        const A mb = Fb.rho + W.un * Fb.p + Wt.un * hp + es * Fb.un + q * he + W.ut * Fb.ut + Wt.ut * hu;
+        const A mtb = hr + W.un * hp + es * he + W.ut * hu;
+        const A esb = m * Fb.un + mt * he, qb = m * he;
+        Wb.rho = Wt.un * mtb + W.un * mb;
+        Wb.p = Fb.p + W.un * Fb.un + Wt.un * he;
+        Wb.un = m * Fb.p + mt * hp + W.p * Fb.un + Wt.p * he + Wt.un * qb + W.un * esb + Wt.rho * mtb + W.rho * mb;
+        Wb.ut = m * Fb.ut + mt * hu + Wt.ut * qb + W.ut * esb;
+        Wb.e = esb;
+        Wtb.rho = W.un * mtb;
+        Wtb.p = hp + W.un * he;
+        Wtb.un = m * hp + W.p * he + W.un * qb + W.rho * mtb;
+        Wtb.ut = m * hu + W.ut * qb;
+        Wtb.e = qb;
     }
     // ---- reverse: Hoisted::grp ----
     A rho_lb = 0, pi_lb = 0, u_lb = 0, v_lb = 0, rho_rb = 0, pi_rb = 0, u_rb = 0, v_rb = 0;
@@ -262,278 +240,209 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
     A irlb = 0, irrb = 0, e_lb = 0, e_rb = 0, e_lxb = 0, e_rxb = 0, c_lxb = 0, c_rxb = 0;
     A c_lb = 0, c_rb = 0, iclb = 0, icrb = 0, slb = 0, srb = 0, dub = 0;
     if (wave == 0) {
-        rho_lb += Wb.rho;
-        pi_lb += Wb.p;
-        u_lb += Wb.un;
+        // W = left face state; Wt: rho_t = -rho_l u_lx - u_l rho_lx, un_t = -u_l u_lx - pi_lx irl,
+        // e_t = -u_l e_lx - pi_l irl u_lx, ut_t = -u_l v_lx, p_t = -u_l pi_lx - c_l sl u_lx
+        const A tp = -Wtb.p, te = -Wtb.e, tn = -Wtb.un, tr = -Wtb.rho;
+        rho_lb += Wb.rho + u_lx * tr;
+        pi_lb += Wb.p + irl * u_lx * te;
+        u_lb += Wb.un + pi_lx * tp - v_lx * Wtb.ut + e_lx * te + u_lx * tn + rho_lx * tr;
         v_lb += Wb.ut;
         e_lb += Wb.e;
-        // p_t = -u_l pi_lx - c_l sl u_lx
-        u_lb += -pi_lx * Wtb.p;
-        pi_lxb += -u_l * Wtb.p;
-        c_lb += -sl * u_lx * Wtb.p;
-        slb += -c_l * u_lx * Wtb.p;
-        u_lxb += -c_l * sl * Wtb.p;
-        // ut_t = -u_l v_lx
-        u_lb += -v_lx * Wtb.ut;
+        pi_lxb += u_l * tp + irl * tn;
+        c_lb += sl * u_lx * tp;
+        slb += c_l * u_lx * tp;
+        u_lxb += c_l * sl * tp + pi_l * irl * te + u_l * tn + rho_l * tr;
         v_lxb += -u_l * Wtb.ut;
-        // e_t = -u_l e_lx - pi_l irl u_lx
-        u_lb += -e_lx * Wtb.e;
-        e_lxb += -u_l * Wtb.e;
-        pi_lb += -irl * u_lx * Wtb.e;
-        irlb += -pi_l * u_lx * Wtb.e;
-        u_lxb += -pi_l * irl * Wtb.e;
-        // un_t = -u_l u_lx - pi_lx irl
-        u_lb += -u_lx * Wtb.un;
-        u_lxb += -u_l * Wtb.un;
-        pi_lxb += -irl * Wtb.un;
-        irlb += -pi_lx * Wtb.un;
-        // rho_t = -rho_l u_lx - u_l rho_lx
-        rho_lb += -u_lx * Wtb.rho;
-        u_lxb += -rho_l * Wtb.rho;
-        u_lb += -rho_lx * Wtb.rho;
-        rho_lxb += -u_l * Wtb.rho;
+        e_lxb += u_l * te;
+        irlb += pi_l * u_lx * te + pi_lx * tn;
+        rho_lxb += u_l * tr;
     } else if (wave == 1) {
-        rho_rb += Wb.rho;
-        pi_rb += Wb.p;
-        u_rb += Wb.un;
+        const A tp = -Wtb.p, te = -Wtb.e, tn = -Wtb.un, tr = -Wtb.rho;
+        rho_rb += Wb.rho + u_rx * tr;
+        pi_rb += Wb.p + irr * u_rx * te;
+        u_rb += Wb.un + pi_rx * tp - v_rx * Wtb.ut + e_rx * te + u_rx * tn + rho_rx * tr;
         v_rb += Wb.ut;
         e_rb += Wb.e;
-        u_rb += -pi_rx * Wtb.p;
-        pi_rxb += -u_r * Wtb.p;
-        c_rb += -sr * u_rx * Wtb.p;
-        srb += -c_r * u_rx * Wtb.p;
-        u_rxb += -c_r * sr * Wtb.p;
-        u_rb += -v_rx * Wtb.ut;
+        pi_rxb += u_r * tp + irr * tn;
+        c_rb += sr * u_rx * tp;
+        srb += c_r * u_rx * tp;
+        u_rxb += c_r * sr * tp + pi_r * irr * te + u_r * tn + rho_r * tr;
         v_rxb += -u_r * Wtb.ut;
-        u_rb += -e_rx * Wtb.e;
-        e_rxb += -u_r * Wtb.e;
-        pi_rb += -irr * u_rx * Wtb.e;
-        irrb += -pi_r * u_rx * Wtb.e;
-        u_rxb += -pi_r * irr * Wtb.e;
-        u_rb += -u_rx * Wtb.un;
-        u_rxb += -u_r * Wtb.un;
-        pi_rxb += -irr * Wtb.un;
-        irrb += -pi_rx * Wtb.un;
-        rho_rb += -u_rx * Wtb.rho;
-        u_rxb += -rho_r * Wtb.rho;
-        u_rb += -rho_rx * Wtb.rho;
-        rho_rxb += -u_r * Wtb.rho;
+        e_rxb += u_r * te;
+        irrb += pi_r * u_rx * te + pi_rx * tn;
+        rho_rxb += u_r * tr;
     } else {
-        A ub = Wb.un, pmb = Wb.p, rhob = Wb.rho, eb = Wb.e;
-        A isumb = 0, k_lb = 0, k_rb = 0, Dpb = 0, urhob = 0, rho3b = 0, irhob = 0, ic2b = 0;
-        A A1b = 0, B1b = 0, C1b = 0, Pb = 0, Vb = 0, Qb = 0, T1b = 0, T2b = 0;
-        A p_tb = Wtb.p;
-        if (star_right) {
-            v_rb += Wb.ut;
-            // ut_t = -urho irr v_rx
-            urhob += -irr * v_rx * Wtb.ut;
-            irrb += -urho * v_rx * Wtb.ut;
-            v_rxb += -urho * irr * Wtb.ut;
-            // e_t = -urho irr Q + pm ic2 p_t
-            urhob += -irr * Q * Wtb.e;
-            irrb += -urho * Q * Wtb.e;
-            Qb += -urho * irr * Wtb.e;
-            pmb += ic2 * Wt.p * Wtb.e;
-            ic2b += pm * Wt.p * Wtb.e;
-            p_tb += pm * ic2 * Wtb.e;
-            // Q = e_rx - pi_r pi_rx ic2 + 2 (e_r - e) c_rx icr
-            e_rxb += Qb;
-            pi_rb += -pi_rx * ic2 * Qb;
-            pi_rxb += -pi_r * ic2 * Qb;
-            ic2b += -pi_r * pi_rx * Qb;
-            e_rb += two * c_rx * icr * Qb;
-            eb += -two * c_rx * icr * Qb;
-            c_rxb += two * (e_r - W.e) * icr * Qb;
-            icrb += two * (e_r - W.e) * c_rx * Qb;
-            // un_t = isum (sl A1 k_l + sr B1 k_r)
-            isumb += (sl * A1 * k_l + sr * B1 * k_r) * Wtb.un;
-            slb += isum * A1 * k_l * Wtb.un;
-            A1b += isum * sl * k_l * Wtb.un;
-            k_lb += isum * sl * A1 * Wtb.un;
-            srb += isum * B1 * k_r * Wtb.un;
-            B1b += isum * sr * k_r * Wtb.un;
-            k_rb += isum * sr * B1 * Wtb.un;
-            // B1 = 1 - urho c_l ic2
-            urhob += -c_l * ic2 * B1b;
-            c_lb += -urho * ic2 * B1b;
-            ic2b += -urho * c_l * B1b;
-        } else {
-            v_lb += Wb.ut;
-            urhob += -irl * v_lx * Wtb.ut;
-            irlb += -urho * v_lx * Wtb.ut;
-            v_lxb += -urho * irl * Wtb.ut;
-            urhob += -irl * Q * Wtb.e;
-            irlb += -urho * Q * Wtb.e;
-            Qb += -urho * irl * Wtb.e;
-            pmb += ic2 * Wt.p * Wtb.e;
-            ic2b += pm * Wt.p * Wtb.e;
-            p_tb += pm * ic2 * Wtb.e;
-            // Q = e_lx - pi_l pi_lx ic2 + 2 (e_l - e) c_lx icl
-            e_lxb += Qb;
-            pi_lb += -pi_lx * ic2 * Qb;
-            pi_lxb += -pi_l * ic2 * Qb;
-            ic2b += -pi_l * pi_lx * Qb;
-            e_lb += two * c_lx * icl * Qb;
-            eb += -two * c_lx * icl * Qb;
-            c_lxb += two * (e_l - W.e) * icl * Qb;
-            iclb += two * (e_l - W.e) * c_lx * Qb;
-            // un_t = isum (sl B1 k_l + sr C1 k_r), B1 = 1 + urho c_r ic2
-            isumb += (sl * B1 * k_l + sr * C1 * k_r) * Wtb.un;
-            slb += isum * B1 * k_l * Wtb.un;
-            B1b += isum * sl * k_l * Wtb.un;
-            k_lb += isum * sl * B1 * Wtb.un;
-            srb += isum * C1 * k_r * Wtb.un;
-            C1b += isum * sr * k_r * Wtb.un;
-            k_rb += isum * sr * C1 * Wtb.un;
-            urhob += c_r * ic2 * B1b;
-            c_rb += urho * ic2 * B1b;
-            ic2b += urho * c_r * B1b;
-        }
-        // p_t = isum (c_r sl A1 k_l - c_l sr C1 k_r)   (both star cases)
-        isumb += (c_r * sl * A1 * k_l - c_l * sr * C1 * k_r) * p_tb;
-        c_rb += isum * sl * A1 * k_l * p_tb;
-        slb += isum * c_r * A1 * k_l * p_tb;
-        A1b += isum * c_r * sl * k_l * p_tb;
-        k_lb += isum * c_r * sl * A1 * p_tb;
-        c_lb += -isum * sr * C1 * k_r * p_tb;
-        srb += -isum * c_l * C1 * k_r * p_tb;
-        C1b += -isum * c_l * sr * k_r * p_tb;
-        k_rb += -isum * c_l * sr * C1 * p_tb;
-        // A1 = 1 + urho icr ; C1 = 1 - urho icl
+        // The star state's side s (right if u <= 0, else left), written once for
+        // both sides with sg = +1 (right) or -1 (left):
+        //   irho = (sg (u_s - u) + s_s) ic_s, rho = 1/irho, ic2 = ic_s^2,
+        //   e = e_s + (pm^2 - pi_s^2)/2 ic2, rho3 = rho^3, urho = u rho,
+        //   P = s_s^2 rho_sx - sg c_s u_sx + 1.5 (u - u_s) c_sx, V = u + sg c_s irho,
+        //   T1 = rho3 ir_s ic2, T2 = rho3 ic2 ic_s, Q = e_sx - pi_s pi_sx ic2 + 2 (e_s - e) c_sx ic_s,
+        //   rho_t = -u T1 P + sg T2 V Dp, e_t = -urho ir_s Q + pm ic2 p_t, ut_t = -urho ir_s v_sx,
+        //   p_t = isum (c_r sl A1 k_l - c_l sr C1 k_r), A1 = 1 + urho icr, C1 = 1 - urho icl,
+        //   un_t = isum (sl a k_l + sr b k_r), with (a, b) = (A1, B1) on the right and (B1, C1)
+        //   on the left, B1 = 1 - sg urho c_o ic2 (c_o the other side's c).
+        const bool R = star_right;
+        const A sg = R ? one : -one;
+        const A u_s = R ? u_r : u_l, s_s = R ? sr : sl, ic_s = R ? icr : icl, ir_s = R ? irr : irl;
+        const A c_s = R ? c_r : c_l, c_o = R ? c_l : c_r, pi_s = R ? pi_r : pi_l, pi_sx = R ? pi_rx : pi_lx;
+        const A e_s = R ? e_r : e_l, c_sx = R ? c_rx : c_lx, rho_sx = R ? rho_rx : rho_lx;
+        const A u_sx = R ? u_rx : u_lx, v_sx = R ? v_rx : v_lx;
+        A ub = Wb.un, pmb = Wb.p, rhob = Wb.rho, eb = Wb.e, p_tb = Wtb.p, Dpb = 0;
+        A k_lb = 0, k_rb = 0, urhob = 0, ic2b = 0, ir_sb = 0, ic_sb = 0, c_sb = 0, c_ob = 0;
+        A u_sb = 0, s_sb = 0, pi_sb = 0, pi_sxb = 0, e_sb = 0, e_sxb = 0, c_sxb = 0, rho_sxb = 0, u_sxb = 0;
+        const A v_sxb = -urho * ir_s * Wtb.ut;
+        // ut_t and e_t
+        const A tt = -(v_sx * Wtb.ut + Q * Wtb.e);
+        urhob += ir_s * tt;
+        ir_sb += urho * tt;
+        const A Qb = -urho * ir_s * Wtb.e;
+        const A cpe = Wt.p * Wtb.e;
+        pmb += ic2 * cpe;
+        ic2b += pm * cpe;
+        p_tb += pm * ic2 * Wtb.e;
+        // Q
+        e_sxb += Qb;
+        const A dq = -ic2 * Qb;
+        pi_sb += pi_sx * dq;
+        pi_sxb += pi_s * dq;
+        ic2b += -pi_s * pi_sx * Qb;
+        const A fq = two * c_sx * ic_s * Qb;
+        e_sb += fq;
+        eb -= fq;
+        const A gq = two * (e_s - W.e) * Qb;
+        c_sxb += ic_s * gq;
+        ic_sb += c_sx * gq;
+        // un_t
+        const A iu = isum * Wtb.un;
+        const A a = R ? A1 : B1, b = R ? B1 : C1;
+        slb += a * k_l * iu;
+        k_lb += sl * a * iu;
+        srb += b * k_r * iu;
+        k_rb += sr * b * iu;
+        const A ab = sl * k_l * iu, bb = sr * k_r * iu;
+        A A1b = R ? ab : A(0), C1b = R ? A(0) : bb;
+        const A B1b = R ? bb : ab;
+        const A hb = -sg * B1b;  // B1 = 1 - sg urho c_o ic2
+        urhob += c_o * ic2 * hb;
+        c_ob += urho * ic2 * hb;
+        ic2b += urho * c_o * hb;
+        // p_t
+        const A ip = isum * p_tb;
+        const A LL = c_r * sl, L2 = A1 * k_l, RR = c_l * sr, R2 = C1 * k_r;
+        const A x1 = ip * L2, x2 = ip * LL, x3 = -ip * R2, x4 = -ip * RR;
+        c_rb += sl * x1;
+        slb += c_r * x1;
+        A1b += k_l * x2;
+        k_lb += A1 * x2;
+        c_lb += sr * x3;
+        srb += c_l * x3;
+        C1b += k_r * x4;
+        k_rb += C1 * x4;
         urhob += icr * A1b - icl * C1b;
         icrb += urho * A1b;
-        iclb += -urho * C1b;
-        if (star_right) {
-            // rho_t = -u T1 P + T2 V Dp
-            ub += -T1 * P * Wtb.rho;
-            T1b += -u * P * Wtb.rho;
-            Pb += -u * T1 * Wtb.rho;
-            T2b += V * Dp * Wtb.rho;
-            Vb += T2 * Dp * Wtb.rho;
-            Dpb += T2 * V * Wtb.rho;
-            // T1 = rho3 irr ic2 ; T2 = rho3 ic2 icr
-            rho3b += irr * ic2 * T1b + ic2 * icr * T2b;
-            irrb += rho3 * ic2 * T1b;
-            ic2b += rho3 * irr * T1b + rho3 * icr * T2b;
-            icrb += rho3 * ic2 * T2b;
-            // P = sr^2 rho_rx - c_r u_rx + 1.5 (u - u_r) c_rx
-            srb += two * sr * rho_rx * Pb;
-            rho_rxb += sr * sr * Pb;
-            c_rb += -u_rx * Pb;
-            u_rxb += -c_r * Pb;
-            ub += onehalf * c_rx * Pb;
-            u_rb += -onehalf * c_rx * Pb;
-            c_rxb += onehalf * (u - u_r) * Pb;
-            // V = u + c_r irho
-            ub += Vb;
-            c_rb += irho * Vb;
-            irhob += c_r * Vb;
-        } else {
-            // rho_t = -u T1 P - T2 V Dp
-            ub += -T1 * P * Wtb.rho;
-            T1b += -u * P * Wtb.rho;
-            Pb += -u * T1 * Wtb.rho;
-            T2b += -V * Dp * Wtb.rho;
-            Vb += -T2 * Dp * Wtb.rho;
-            Dpb += -T2 * V * Wtb.rho;
-            // T1 = rho3 irl ic2 ; T2 = rho3 ic2 icl
-            rho3b += irl * ic2 * T1b + ic2 * icl * T2b;
-            irlb += rho3 * ic2 * T1b;
-            ic2b += rho3 * irl * T1b + rho3 * icl * T2b;
-            iclb += rho3 * ic2 * T2b;
-            // P = sl^2 rho_lx + c_l u_lx + 1.5 (u - u_l) c_lx
-            slb += two * sl * rho_lx * Pb;
-            rho_lxb += sl * sl * Pb;
-            c_lb += u_lx * Pb;
-            u_lxb += c_l * Pb;
-            ub += onehalf * c_lx * Pb;
-            u_lb += -onehalf * c_lx * Pb;
-            c_lxb += onehalf * (u - u_l) * Pb;
-            // V = u - c_l irho
-            ub += Vb;
-            c_lb += -irho * Vb;
-            irhob += -c_l * Vb;
-        }
-        // urho = u rho ; rho3 = rho^3
+        iclb -= urho * C1b;
+        // rho_t
+        const A y1 = -Wtb.rho * T1, y2 = sg * Wtb.rho * T2;
+        ub += P * y1;
+        const A Pb = u * y1, Vb = Dp * y2;
+        Dpb += V * y2;
+        const A T1b = -u * P * Wtb.rho, T2b = sg * V * Dp * Wtb.rho;
+        const A zt = ir_s * T1b + ic_s * T2b, w = rho3 * ic2;
+        A rho3b = ic2 * zt;
+        ic2b += rho3 * zt;
+        ir_sb += w * T1b;
+        ic_sb += w * T2b;
+        // P
+        s_sb += two * s_s * rho_sx * Pb;
+        rho_sxb += s_s * s_s * Pb;
+        c_sb += -sg * u_sx * Pb;
+        u_sxb += -sg * c_s * Pb;
+        const A kp = onehalf * c_sx * Pb;
+        ub += kp;
+        u_sb -= kp;
+        c_sxb += onehalf * (u - u_s) * Pb;
+        // V
+        ub += Vb;
+        c_sb += sg * irho * Vb;
+        A irhob = sg * c_s * Vb;
+        // urho, rho3
         ub += rho * urhob;
         rhob += u * urhob + A(3) * rho * rho * rho3b;
-        if (star_right) {
-            // e = e_r + (pm^2 - pi_r^2)/2 ic2
-            e_rb += eb;
-            pmb += pm * ic2 * eb;
-            pi_rb += -pi_r * ic2 * eb;
-            ic2b += half * (pm * pm - pi_r * pi_r) * eb;
-            // ic2 = icr^2
-            icrb += two * icr * ic2b;
-            // rho = 1/irho ; irho = (u_r - u + sr) icr
-            irhob += -rho * rho * rhob;
-            u_rb += icr * irhob;
-            ub += -icr * irhob;
-            srb += icr * irhob;
-            icrb += (u_r - u + sr) * irhob;
+        // e, ic2
+        e_sb += eb;
+        pmb += pm * ic2 * eb;
+        pi_sb -= pi_s * ic2 * eb;
+        ic2b += half * (pm * pm - pi_s * pi_s) * eb;
+        ic_sb += two * ic_s * ic2b;
+        // rho = 1/irho, irho = (sg (u_s - u) + s_s) ic_s
+        irhob -= rho * rho * rhob;
+        const A vi = ic_s * irhob;
+        u_sb += sg * vi;
+        ub -= sg * vi;
+        s_sb += vi;
+        ic_sb += (sg * (u_s - u) + s_s) * irhob;
+        // back to the two sides
+        if (R) {
+            v_rb += Wb.ut; v_rxb += v_sxb; u_rb += u_sb; srb += s_sb; icrb += ic_sb; irrb += ir_sb;
+            c_rb += c_sb; c_lb += c_ob; pi_rb += pi_sb; pi_rxb += pi_sxb; e_rb += e_sb; e_rxb += e_sxb;
+            c_rxb += c_sxb; rho_rxb += rho_sxb; u_rxb += u_sxb;
         } else {
-            e_lb += eb;
-            pmb += pm * ic2 * eb;
-            pi_lb += -pi_l * ic2 * eb;
-            ic2b += half * (pm * pm - pi_l * pi_l) * eb;
-            iclb += two * icl * ic2b;
-            // irho = (u - u_l + sl) icl
-            irhob += -rho * rho * rhob;
-            ub += icl * irhob;
-            u_lb += -icl * irhob;
-            slb += icl * irhob;
-            iclb += (u - u_l + sl) * irhob;
+            v_lb += Wb.ut; v_lxb += v_sxb; u_lb += u_sb; slb += s_sb; iclb += ic_sb; irlb += ir_sb;
+            c_lb += c_sb; c_rb += c_ob; pi_lb += pi_sb; pi_lxb += pi_sxb; e_lb += e_sb; e_lxb += e_sxb;
+            c_lxb += c_sxb; rho_lxb += rho_sxb; u_lxb += u_sxb;
         }
         // Dp = (c_r d_l - c_l d_r) isum / 2
-        c_rb += d_l * half * isum * Dpb;
-        c_lb += -d_r * half * isum * Dpb;
-        A d_lb = c_r * half * isum * Dpb, d_rb = -c_l * half * isum * Dpb;
-        isumb += (c_r * d_l - c_l * d_r) * half * Dpb;
+        const A hD = half * isum * Dpb;
+        c_rb += d_l * hD;
+        c_lb -= d_r * hD;
+        const A d_lb = c_r * hD, d_rb = -c_l * hD;
         // d_r = sr G ; G = 2 (c_r u_rx - pi_rx) + u_r c_rx
         srb += G * d_rb;
         const A Gb = sr * d_rb;
         c_rb += two * u_rx * Gb;
         u_rxb += two * c_r * Gb;
-        pi_rxb += -two * Gb;
+        pi_rxb -= two * Gb;
         u_rb += c_rx * Gb;
         c_rxb += u_r * Gb;
         // d_l = sl H ; H = -2 (c_l u_lx + pi_lx) - u_l c_lx
         slb += H * d_lb;
         const A Hb = sl * d_lb;
-        c_lb += -two * u_lx * Hb;
-        u_lxb += -two * c_l * Hb;
-        pi_lxb += -two * Hb;
-        u_lb += -c_lx * Hb;
-        c_lxb += -u_l * Hb;
-        // k_r = -pi_rx + c_r u_rx + u_r c_rx / 2
-        pi_rxb += -k_rb;
+        c_lb -= two * u_lx * Hb;
+        u_lxb -= two * c_l * Hb;
+        pi_lxb -= two * Hb;
+        u_lb -= c_lx * Hb;
+        c_lxb -= u_l * Hb;
+        // k_r = -pi_rx + c_r u_rx + u_r c_rx / 2 ; k_l = -pi_lx - c_l u_lx - u_l c_lx / 2
+        pi_rxb -= k_rb;
         c_rb += u_rx * k_rb;
         u_rxb += c_r * k_rb;
         u_rb += half * c_rx * k_rb;
         c_rxb += half * u_r * k_rb;
-        // k_l = -pi_lx - c_l u_lx - u_l c_lx / 2
-        pi_lxb += -k_lb;
-        c_lb += -u_lx * k_lb;
-        u_lxb += -c_l * k_lb;
-        u_lb += -half * c_lx * k_lb;
-        c_lxb += -half * u_l * k_lb;
+        pi_lxb -= k_lb;
+        c_lb -= u_lx * k_lb;
+        u_lxb -= c_l * k_lb;
+        u_lb -= half * c_lx * k_lb;
+        c_lxb -= half * u_l * k_lb;
         // pm = (du c_l c_r + c_l pi_r + c_r pi_l) isum
-        dub += c_l * c_r * isum * pmb;
-        c_lb += (du * c_r + pi_r) * isum * pmb;
-        c_rb += (du * c_l + pi_l) * isum * pmb;
-        pi_rb += c_l * isum * pmb;
-        pi_lb += c_r * isum * pmb;
-        isumb += (du * c_l * c_r + c_l * pi_r + c_r * pi_l) * pmb;
+        const A ipm = isum * pmb;
+        dub += c_l * c_r * ipm;
+        c_lb += (du * c_r + pi_r) * ipm;
+        c_rb += (du * c_l + pi_l) * ipm;
+        pi_rb += c_l * ipm;
+        pi_lb += c_r * ipm;
         // u = (u_l c_l + u_r c_r + pi_l - pi_r) isum
-        u_lb += c_l * isum * ub;
-        c_lb += u_l * isum * ub;
-        u_rb += c_r * isum * ub;
-        c_rb += u_r * isum * ub;
-        pi_lb += isum * ub;
-        pi_rb += -isum * ub;
-        isumb += (u_l * c_l + u_r * c_r + pi_l - pi_r) * ub;
-        // isum = 1/(c_l + c_r)
-        const A sb = -isum * isum * isumb;
+        const A iub = isum * ub;
+        u_lb += c_l * iub;
+        c_lb += u_l * iub;
+        u_rb += c_r * iub;
+        c_rb += u_r * iub;
+        pi_lb += iub;
+        pi_rb -= iub;
+        // isum = 1/(c_l + c_r): each quantity X = bracket isum above gives
+        // bracket * Xb = X (c_l + c_r) Xb to isum's adjoint, and
+        // d isum / d c = -isum^2, so c_l and c_r receive -isum sum(X Xb)
+        const A sb = -isum * (u * ub + pm * pmb + Wt.p * p_tb + Wt.un * Wtb.un + Dp * Dpb);
         c_lb += sb;
         c_rb += sb;
     }
