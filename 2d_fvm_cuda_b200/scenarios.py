@@ -246,17 +246,22 @@ def shock_bubble(nx: int, ny: int, width: float = 2.0, height: float = 1.0, seed
     hx, hy = width / nx, height / ny
     xs = (np.arange(nx) + 0.5) * hx
     ys = height - (np.arange(ny) + 0.5) * hy
-    frac = np.zeros((ny, nx))
     offs = (np.arange(sub) + 0.5) / sub - 0.5
+    # cells whose every sub-sample lies on one side of the perturbed edge
+    # (radius within radius (1 +- amplitude)) are 0 or 1; only the band between
+    # is sub-sampled
+    d = np.hypot(xs[None, :] - centre[0], ys[:, None] - centre[1])
+    reach = hx + hy
+    frac = (d + reach < radius * (1.0 - amplitude)).astype(np.float64)
+    jb, ib = np.nonzero((d + reach >= radius * (1.0 - amplitude)) & (d - reach <= radius * (1.0 + amplitude)))
+    count = np.zeros(jb.size)
     for ox in offs:
         for oy in offs:
-            X = xs[None, :] + ox * hx
-            Y = ys[:, None] + oy * hy
-            dx, dy = X - centre[0], Y - centre[1]
+            dx, dy = xs[ib] + ox * hx - centre[0], ys[jb] + oy * hy - centre[1]
             th = np.arctan2(dy, dx)
             r = radius * (1.0 + sum(a[k] * np.cos((k + 1) * th + ph[k]) for k in range(modes)))
-            frac += (dx * dx + dy * dy < r * r)
-    frac /= sub * sub
+            count += (dx * dx + dy * dy < r * r)
+    frac[jb, ib] = count / (sub * sub)
     U = np.empty((ny, nx, 4))
     U[..., 0] = rho_bubble * frac + 1.0 * (1.0 - frac)
     U[..., 1] = 1.0

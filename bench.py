@@ -508,6 +508,38 @@ def form_vortex(args):
     return {"form": "vortex", "workload": "2000^2 periodic isentropic vortex, one period", "results": res}
 
 
+def form_precision(args):
+    """Precision form: 4096^2 Mach-2 shock hitting a light bubble (rho 0.1,
+    radius 0.15, 8 seeded boundary modes of total amplitude <= 0.01) in a
+    [0,2]x[0,1] channel, reflective top/bottom, transmissive left/right,
+    t_end 0.4, CFL 0.45: the FP32 build (compensated update, FP64 dt) against
+    the FP64 build, density L1 and Linf, and their speeds."""
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    n = args.n
+    U0 = pkg.scenarios.shock_bubble(n, n, width=2.0, height=1.0, seed=0)
+    res, states = {}, {}
+    # FP64_REFORDER (the reference's operation order) differs from FP64 by
+    # rounding only: how far two FP64 runs drift apart on this flow
+    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32"), (pkg.FP64_REFORDER, "fp64_reference_order")):
+        h = pkg.Handle(n, n)
+        h.configure(2.0, 1.0, 0.4, 0.45, 1.9, 1.4, 6, prec)
+        h.set_state(U0)
+        h.solve()
+        ms, _ = h.run_stats()
+        t, steps, _ = h.time()
+        states[name] = h.get_state(4)[..., 0]
+        h.close()
+        res[name] = {"steps": steps, "t": t, "device_s": ms / 1e3, "cell_updates_per_s": n * n * steps / (ms / 1e3)}
+    D, S = states["fp64"], states["fp32"]
+    res["fp32"]["rho_rel_l1_vs_fp64"] = float(np.abs(S - D).sum() / np.abs(D).sum())
+    res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(S - D).max())
+    res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
+    Rf = states["fp64_reference_order"]
+    res["fp64_reference_order"]["rho_rel_l1_vs_fp64"] = float(np.abs(Rf - D).sum() / np.abs(D).sum())
+    res["fp64_reference_order"]["rho_linf_vs_fp64"] = float(np.abs(Rf - D).max())
+    return {"form": "precision", "workload": f"{n}^2 Mach-2 shock-bubble, [0,2]x[0,1], t_end 0.4", "results": res}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,7 +551,7 @@ def main():
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="arithmetic of a --kernels-only run")
-    ap.add_argument("--form", choices=["batch", "adjoint", "vortex"],
+    ap.add_argument("--form", choices=["batch", "adjoint", "vortex", "precision"],
                     help="measure one of the other forms instead (one JSON line, rank 0, one GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -527,7 +559,8 @@ def main():
     rank, world, local_rank = rank_info()
     if args.form:
         if rank == 0:
-            print(json.dumps({"batch": form_batch, "adjoint": form_adjoint, "vortex": form_vortex}[args.form](args)),
+            print(json.dumps({"batch": form_batch, "adjoint": form_adjoint, "vortex": form_vortex,
+                              "precision": form_precision}[args.form](args)),
                   flush=True)
         return
     if args.impl == "reference":
