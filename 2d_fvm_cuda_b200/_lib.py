@@ -39,6 +39,10 @@ SIGNATURES = [
     ("fvm2d_get_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     ("fvm2d_solve", ctypes.c_int, [_vp]),
     ("fvm2d_advance", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_set_record_model", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
+    ("fvm2d_write_frame_png", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("fvm2d_write_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("fvm2d_read_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("fvm2d_advance_dt", ctypes.c_int, [_vp, ctypes.c_double]),
     ("fvm2d_get_wave_speed_max", ctypes.c_int, [_vp, _dp]),
     ("fvm2d_set_row_frame", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -198,6 +202,21 @@ class Handle:
         k = ctypes.c_int(0)
         check(self.lib.fvm2d_profile_kernels(self.h, int(nsteps), out, ctypes.byref(k)))
         return list(out), k.value
+
+    # -- frames and state files --
+    def set_record_model(self, on: bool, gap_per_frame: int = 10, record_dir: str = ".") -> None:
+        """Frames <record_dir>/<k>.png during solve(), every gap_per_frame steps."""
+        check(self.lib.fvm2d_set_record_model(self.h, int(bool(on)), int(gap_per_frame),
+                                              os.fsencode(record_dir)))
+
+    def write_frame_png(self, path: str) -> None:
+        check(self.lib.fvm2d_write_frame_png(self.h, os.fsencode(path)))
+
+    def write_state(self, path: str) -> None:
+        check(self.lib.fvm2d_write_state(self.h, os.fsencode(path)))
+
+    def read_state(self, path: str) -> None:
+        check(self.lib.fvm2d_read_state(self.h, os.fsencode(path)))
 
     # -- row slabs (one problem split across processes) --
     def advance_dt(self, dt: float) -> None:

@@ -11,6 +11,7 @@
 //   is one 64-byte read per graph replay (the reference reads the max wave
 //   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
 #include "../../include/fvm2d.h"
+#include "fvm2d_io.cuh"
 #include "fvm2d_adjoint.h"
 #include "fvm2d_control.h"
 #include "fvm2d_dual.cuh"
@@ -20,6 +21,7 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <new>
 #include <string>
 #include <utility>
@@ -121,6 +123,9 @@ struct fvm2d_solver {
     bool need_init = true;
     double fixed_dt = 0.0;        // > 0: differentiation runs step with this constant dt
     int row0 = 0, ny_global = 0, fill_top = 1, fill_bottom = 1;  // row frame of a slab (fvm2d_set_row_frame)
+    bool record_on = false;       // frames during fvm2d_solve (fvm2d_set_record_model)
+    int record_gap = 10;
+    std::string record_dir = ".";
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
     double *ckpt = nullptr;       // checkpoints of fvm2d_forward
@@ -477,6 +482,59 @@ int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride)
     return FVM2D_OK;
 }
 
+static int write_frame(fvm2d_solver *s, const char *path);
+
+// fvm2d_solve with frames: one after the first step, then one every `gap`
+// steps, named by the index of the step they follow (src/wrappers.cuh:
+// 194-195, 253-263); the frame shows the state after that step's ghost fill.
+static int solve_recording(fvm2d_solver *s)
+{
+    std::error_code ec;
+    std::filesystem::create_directories(s->record_dir, ec);
+    StepControl *c = s->ctl_h;
+    const LaunchConfig cfg = s->config();
+    auto t0 = std::chrono::high_resolution_clock::now();
+    double device_ms = 0.0;
+    long long launches = 0;
+    int target = 1;
+    c->step_limit = target;
+    if (int rc = s->upload_control()) return rc;
+    CK(cudaEventRecord(s->ev_begin, s->stream));
+    CK(kVariants[s->precision].init(cfg, s->stream));
+    s->need_init = false;
+    for (;;) {
+        if (int rc = s->loop(1, target - c->steps)) return rc;
+        device_ms += s->last_device_ms;
+        launches += s->last_launches;
+        if (c->steps == target) {
+            const std::string path = s->record_dir + "/" + std::to_string(target - 1) + ".png";
+            if (int rc = write_frame(s, path.c_str())) return rc;
+        }
+        if (c->done || c->steps < target || s->record_gap <= 0) break;
+        target += s->record_gap;
+        c->step_limit = target;
+        c->active = 0;
+        if (int rc = s->upload_control()) return rc;
+        CK(cudaEventRecord(s->ev_begin, s->stream));
+        CK(kVariants[s->precision].plan(cfg, s->stream));
+    }
+    if (s->record_gap <= 0 && !c->done) {  // the reference records only its first step then
+        c->step_limit = INT_MAX;
+        c->active = 0;
+        if (int rc = s->upload_control()) return rc;
+        CK(cudaEventRecord(s->ev_begin, s->stream));
+        CK(kVariants[s->precision].plan(cfg, s->stream));
+        if (int rc = s->loop(1, LLONG_MAX)) return rc;
+        device_ms += s->last_device_ms;
+        launches += s->last_launches;
+    }
+    auto t1 = std::chrono::high_resolution_clock::now();
+    s->last_ms = std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count() / 1000.0;
+    s->last_device_ms = device_ms;
+    s->last_launches = launches;
+    return FVM2D_OK;
+}
+
 int fvm2d_solve(fvm2d_solver *s)
 {
     if (int rc = check(s)) return rc;
@@ -484,9 +542,14 @@ int fvm2d_solve(fvm2d_solver *s)
     StepControl *c = s->ctl_h;
     std::memset(c, 0, sizeof(StepControl));
     c->step_limit = INT_MAX;
-    if (int rc = s->upload_control()) return rc;
     const LaunchConfig cfg = s->config();
     if (int rc = s->build_graphs()) return rc;
+    if (s->record_on) {
+        if (int rc = solve_recording(s)) return rc;
+        s->total_steps += c->steps;
+        return FVM2D_OK;
+    }
+    if (int rc = s->upload_control()) return rc;
     CK(cudaEventRecord(s->ev_begin, s->stream));
     CK(kVariants[s->precision].init(cfg, s->stream));
     s->need_init = false;
@@ -620,6 +683,93 @@ int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows)
         rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
+    return FVM2D_OK;
+}
+
+// ---- frames and state files ---------------------------------------------------
+static int write_frame(fvm2d_solver *s, const char *path)
+{
+    constexpr int NT = 256;
+    const long long n = (long long)s->nx * s->ny;
+    long long blocks = (n + NT - 1) / NT;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    float *parts = reinterpret_cast<float *>(s->scratch);
+    unsigned char *rgb = reinterpret_cast<unsigned char *>(s->scratch) + 4096 * sizeof(float);
+    if (is_fp32(s->precision)) {
+        const float *rho = reinterpret_cast<const float *>(s->U);
+        fvm2d::io::density_range_blocks<float, NT><<<(int)blocks, NT, 0, s->stream>>>(rho, s->pitch, s->nx, s->ny, parts);
+        fvm2d::io::render_density<float><<<148 * 4, 256, 0, s->stream>>>(rho, s->pitch, s->nx, s->ny, parts, (int)blocks,
+                                                                        rgb);
+    } else {
+        fvm2d::io::density_range_blocks<double, NT><<<(int)blocks, NT, 0, s->stream>>>(s->U, s->pitch, s->nx, s->ny, parts);
+        fvm2d::io::render_density<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->pitch, s->nx, s->ny, parts, (int)blocks,
+                                                                         rgb);
+    }
+    CK(cudaGetLastError());
+    std::vector<unsigned char> host((size_t)n * 3);
+    CK(cudaMemcpyAsync(host.data(), rgb, host.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (!fvm2d::io::write_png_rgb(path, s->nx, s->ny, host.data()))
+        return fail(FVM2D_ERR_INVALID, (std::string("cannot write ") + path).c_str());
+    return FVM2D_OK;
+}
+
+int fvm2d_write_frame_png(fvm2d_solver *s, const char *path)
+{
+    if (int rc = check(s)) return rc;
+    if (!path) return fail(FVM2D_ERR_INVALID, "null path");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    return write_frame(s, path);
+}
+
+int fvm2d_set_record_model(fvm2d_solver *s, int on, int gap_per_frame, const char *dir)
+{
+    if (int rc = check(s)) return rc;
+    s->record_on = on != 0;
+    s->record_gap = gap_per_frame;
+    s->record_dir = dir ? dir : ".";
+    return FVM2D_OK;
+}
+
+int fvm2d_write_state(fvm2d_solver *s, const char *path)
+{
+    if (int rc = check(s)) return rc;
+    if (!path) return fail(FVM2D_ERR_INVALID, "null path");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    std::vector<double> cells((size_t)s->nx * s->ny * 4);
+    if (int rc = fvm2d_get_state(s, cells.data(), 4)) return rc;
+    fvm2d::io::StateFileHeader hd;
+    std::memcpy(hd.magic, "FVM2DST1", 8);
+    hd.nx = s->nx;
+    hd.ny = s->ny;
+    hd.t = s->ctl_h->t;
+    hd.steps = s->ctl_h->steps;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(FVM2D_ERR_INVALID, (std::string("cannot open ") + path).c_str());
+    const bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1 &&
+                    std::fwrite(cells.data(), sizeof(double), cells.size(), f) == cells.size();
+    if (std::fclose(f) != 0 || !ok) return fail(FVM2D_ERR_INVALID, (std::string("cannot write ") + path).c_str());
+    return FVM2D_OK;
+}
+
+int fvm2d_read_state(fvm2d_solver *s, const char *path)
+{
+    if (int rc = check(s)) return rc;
+    if (!path) return fail(FVM2D_ERR_INVALID, "null path");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(FVM2D_ERR_INVALID, (std::string("cannot open ") + path).c_str());
+    fvm2d::io::StateFileHeader hd;
+    std::vector<double> cells((size_t)s->nx * s->ny * 4);
+    const bool head = std::fread(&hd, sizeof hd, 1, f) == 1 && std::memcmp(hd.magic, "FVM2DST1", 8) == 0;
+    const bool size = head && hd.nx == s->nx && hd.ny == s->ny;
+    const bool body = size && std::fread(cells.data(), sizeof(double), cells.size(), f) == cells.size();
+    std::fclose(f);
+    if (!head) return fail(FVM2D_ERR_INVALID, "not an fvm2d state file");
+    if (!size) return fail(FVM2D_ERR_INVALID, "the state file's nx, ny differ from the solver's");
+    if (!body) return fail(FVM2D_ERR_INVALID, "the state file is truncated");
+    if (int rc = fvm2d_set_state(s, cells.data(), 4)) return rc;
+    s->ctl_h->t = hd.t;  // fvm2d_advance continues from the saved time and step count
+    s->ctl_h->steps = int(hd.steps);
     return FVM2D_OK;
 }
 

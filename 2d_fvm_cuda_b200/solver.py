@@ -95,9 +95,10 @@ class RGRP_2D_CUDA:
         self._precision = precision(p)
 
     def setRecordModel(self, on_off: bool, gapPerFrame: int = 10, recordDir: str = ".") -> None:
-        """PNG frame recording (src/wrappers.cuh:147-152) is not provided."""
-        if on_off:
-            raise NotImplementedError("frame recording to PNG is not provided by this solver")
+        """PNG frames during solve() (src/wrappers.cuh:147-152): <recordDir>/<k>.png
+        after step k for k = 0, gapPerFrame, 2 gapPerFrame, ..., density in
+        viridis over its range (rendered on the GPU, written without OpenCV)."""
+        self._record = (bool(on_off), int(gapPerFrame), str(recordDir))
 
     # -- solve: src/wrappers.cuh:154-306 ----------------------------------
     def _get_handle(self) -> _lib.Handle:
@@ -108,6 +109,7 @@ class RGRP_2D_CUDA:
             h = self._handle = _lib.Handle(self._nx, self._ny)
         h.configure(self._width, self._height, self._end_time, self._cfl, self._alpha, self._gamma,
                     int(self._strategy), int(self._precision))
+        h.set_record_model(*getattr(self, "_record", (False, 10, ".")))
         return h
 
     def solve(self) -> np.ndarray:

@@ -137,6 +137,25 @@ int fvm2d_solve(fvm2d_solver *s);
  * benchmarks). */
 int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done);
 
+/* ---- frames and state files -----------------------------------------------
+ * Frame recording replaces RGRP_2D_CUDA::setRecordModel / writeStagesTo_png
+ * (src/wrappers.cuh:147-152, 253-260, 323-345): with recording on,
+ * fvm2d_solve writes <dir>/<k>.png after step k for k = 0, gap, 2 gap, ...
+ * (k counts from 0), density mapped to viridis over its min..max range.  The
+ * frame shows the state after the step's ghost fill (the reference's, before
+ * it).  PNG files are written without OpenCV or zlib (stored deflate). */
+int fvm2d_set_record_model(fvm2d_solver *s, int on, int gap_per_frame, const char *dir);
+
+/* The current density as a viridis PNG, as the recorder writes it. */
+int fvm2d_write_frame_png(fvm2d_solver *s, const char *path);
+
+/* State files (no reference counterpart): "FVM2DST1", int32 nx, int32 ny,
+ * double t, int64 steps, then ny*nx cells of (rho, p, u, v) doubles.
+ * fvm2d_read_state needs a solver of the same nx, ny; it sets the state, the
+ * time and the step count, so fvm2d_advance continues the saved run. */
+int fvm2d_write_state(fvm2d_solver *s, const char *path);
+int fvm2d_read_state(fvm2d_solver *s, const char *path);
+
 /* ---- row slabs (no reference counterpart) ---------------------------------
  * One problem split by rows across processes (2d_fvm_cuda_b200/slab.py): each
  * process holds a slab with two halo rows per inner edge, exchanges them

@@ -10,8 +10,8 @@
 // needed).  Differences from the reference, all at the edges of the hot path:
 //  - failures throw std::runtime_error with the library's message (the
 //    reference checks no CUDA call);
-//  - setRecordModel(true, ...) throws: PNG frame recording (OpenCV) is not
-//    provided;
+//  - setRecordModel frames are rendered on the GPU and written without
+//    OpenCV; they show the state after each recorded step's ghost fill;
 //  - ghostCellStrategy gains `periodic` and `reflective_tb`.
 #pragma once
 
@@ -97,9 +97,9 @@ public:
     void setPrecision(int precision) { precision_ = precision; }
     void setRecordModel(bool on_off, int gapPerFrame = 10, const std::string &recordDir = ".")
     {
-        (void)gapPerFrame;
-        (void)recordDir;
-        if (on_off) throw std::runtime_error("frame recording to PNG is not provided by libfvm2d");
+        record_ = on_off;
+        gap_ = gapPerFrame;
+        recordDir_ = recordDir;
     }
 
     std::vector<std::vector<vec5d>> solve()
@@ -117,6 +117,7 @@ public:
         ok(fvm2d_set_gamma(h_, gamma_));
         ok(fvm2d_set_ghost_strategy(h_, (int)strategy_));
         ok(fvm2d_set_precision(h_, precision_));
+        ok(fvm2d_set_record_model(h_, record_ ? 1 : 0, gap_, recordDir_.c_str()));
         ok(fvm2d_set_state(h_, U0_[0].data, 5));
         ok(fvm2d_solve(h_));
         ok(fvm2d_get_computation_time_ms(h_, &ms_));
@@ -160,6 +161,9 @@ protected:
     int Nx_ = 100, Ny_ = 100;
     ghostCellStrategy strategy_ = ghostCellStrategy::outflow;
     int precision_ = FVM2D_FP64;
+    bool record_ = false;
+    int gap_ = 10;
+    std::string recordDir_ = ".";
     double ms_ = 0.0;
     int stages_ = 0;
     fvm2d_solver *h_ = nullptr;
