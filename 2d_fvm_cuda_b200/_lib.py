@@ -35,6 +35,8 @@ SIGNATURES = [
     ("fvm2d_set_ghost_strategy", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fvm2d_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fvm2d_set_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("fvm2d_set_state_planes", ctypes.c_int, [_vp, _vp]),
+    ("fvm2d_get_state_planes", ctypes.c_int, [_vp, _vp]),
     ("fvm2d_set_rp_initial_data", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
     ("fvm2d_get_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     ("fvm2d_solve", ctypes.c_int, [_vp]),
@@ -164,6 +166,24 @@ class Handle:
         assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (self.ny, self.nx, stride)
         check(self.lib.fvm2d_get_state(self.h, out.ctypes.data, stride))
         return out
+
+    def set_state_planes(self, planes) -> None:
+        """Uploads a (4, ny, nx) array of planes rho, p, u, v."""
+        P = np.ascontiguousarray(planes, dtype=np.float64)
+        assert P.shape == (4, self.ny, self.nx)
+        check(self.lib.fvm2d_set_state_planes(self.h, P.ctypes.data))
+
+    def get_state_planes(self) -> np.ndarray:
+        out = np.empty((4, self.ny, self.nx))
+        check(self.lib.fvm2d_get_state_planes(self.h, out.ctypes.data))
+        return out
+
+    def set_state_planes_ptr(self, ptr: int) -> None:
+        """From host or device memory at ptr: 4*ny*nx doubles, planes rho, p, u, v."""
+        check(self.lib.fvm2d_set_state_planes(self.h, ptr))
+
+    def get_state_planes_ptr(self, ptr: int) -> None:
+        check(self.lib.fvm2d_get_state_planes(self.h, ptr))
 
     def get_state_ptr(self, ptr: int, stride: int) -> None:
         check(self.lib.fvm2d_get_state(self.h, ptr, stride))

@@ -443,6 +443,32 @@ int fvm2d_set_state(fvm2d_solver *s, const double *cells, int stride)
     return upload(s, cells, stride);
 }
 
+int fvm2d_set_state_planes(fvm2d_solver *s, const double *planes)
+{
+    if (int rc = check(s)) return rc;
+    if (!planes) return fail(FVM2D_ERR_INVALID, "null state pointer");
+    CK(cudaMemcpyAsync(s->scratch, planes, sizeof(double) * 4 * (size_t)s->nx * s->ny, cudaMemcpyDefault, s->stream));
+    if (is_fp32(s->precision))
+        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, 0, s->ny,
+                                                       s->nx, s->scratch);
+    else
+        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, 0, s->ny, s->nx, s->scratch);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    s->have_state = true;
+    s->need_init = true;
+    std::memset(s->ctl_h, 0, sizeof(StepControl));
+    return FVM2D_OK;
+}
+
+int fvm2d_get_state_planes(fvm2d_solver *s, double *planes)
+{
+    if (int rc = check(s)) return rc;
+    if (!planes) return fail(FVM2D_ERR_INVALID, "null state pointer");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    return fvm2d_get_rows(s, 0, s->ny, planes);
+}
+
 int fvm2d_set_rp_initial_data(fvm2d_solver *s, const double *U1, const double *U2, const double *U3,
                               const double *U4)
 {

@@ -116,6 +116,12 @@ int fvm2d_set_precision(fvm2d_solver *s, int precision);
  * current run to zero. */
 int fvm2d_set_state(fvm2d_solver *s, const double *cells, int stride);
 
+/* The state as four planes, [4][ny][nx] doubles (rho, p, u, v), from or into
+ * host or device memory (a (4, ny, nx) tensor, say).  No reference
+ * counterpart: the reference takes vec5d rows only. */
+int fvm2d_set_state_planes(fvm2d_solver *s, const double *planes);
+int fvm2d_get_state_planes(fvm2d_solver *s, double *planes);
+
 /* setRPInitialData (src/wrappers.cuh:80-108): four constant states (4 doubles
  * each: rho, p, u, v) split at column nx/2 and row ny/2 -- U2 | U1 over U3 | U4. */
 int fvm2d_set_rp_initial_data(fvm2d_solver *s, const double *U1, const double *U2,

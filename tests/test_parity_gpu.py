@@ -219,3 +219,28 @@ def test_invalid_calls_return_errors(pkg):
     with pytest.raises(pkg.FVM2DError):
         h.solve()  # no state yet
     h.close()
+
+
+@pytest.mark.parametrize("precision", [0, 3])
+def test_state_planes_from_host_and_device_memory(pkg, precision):
+    import torch
+
+    nx, ny = 45, 38
+    U = pkg.scenarios.seeded_four_quadrant(nx, ny, 9)
+    P = np.ascontiguousarray(np.moveaxis(U, -1, 0))
+    a, b, c = pkg.Handle(nx, ny), pkg.Handle(nx, ny), pkg.Handle(nx, ny)
+    for h in (a, b, c):
+        h.configure(1.0, 1.0, 0.05, 0.45, 1.9, 1.4, 0, precision)
+    a.set_state(U)
+    b.set_state_planes(P)
+    T = torch.from_numpy(P).cuda()
+    c.set_state_planes_ptr(T.data_ptr())
+    assert np.array_equal(b.get_state(4), a.get_state(4)) and np.array_equal(c.get_state(4), a.get_state(4))
+    for h in (a, b, c):
+        h.solve()
+    assert np.array_equal(b.get_state_planes(), np.moveaxis(a.get_state(4), -1, 0))
+    out = torch.empty((4, ny, nx), dtype=torch.float64, device="cuda")
+    c.get_state_planes_ptr(out.data_ptr())
+    assert np.array_equal(out.cpu().numpy(), np.moveaxis(a.get_state(4), -1, 0))
+    for h in (a, b, c):
+        h.close()
