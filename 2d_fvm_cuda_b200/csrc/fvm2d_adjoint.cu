@@ -55,7 +55,7 @@ __device__ __forceinline__ Cell<A> line_adjoint(const Cell<A> &U, const Cell<A> 
     const bool has_slope = c >= 1 && c <= L - 2;
     const bool iface = c >= 2 && c <= L - 2;
     Cell<A> s = zero_cell();
-    if (has_slope) s = cell_slope(Um, U, Up, K);
+    if (has_slope) s = Hoisted::slope(Um, U, Up, K);
     const Cell<A> sm = shfl_up(s);
     const Cell<A> FR = shfl_down(F);
     // the cell's conservative update

@@ -20,19 +20,17 @@ struct Cell5 {
 };
 
 // ---- limiter -------------------------------------------------------------
-// s = limited_slope(m, c, p): which difference was selected (0 none,
-// 1 central, 2 backward, 3 forward), for the adjoint.  Same tests and tie
-// order as limited_slope.
+// s = Hoisted::slope's limiter (limited_slope_hoisted) on (m, c, p): which
+// difference was selected (0 none, 1 central, 2 backward, 3 forward), for the
+// adjoint.  Same tests and tie order.
 __device__ __forceinline__ int slope_choice(A m, A c, A p, A rh, A alpha)
 {
-    const A central = (p - m) * A(0.5) * rh;
-    const A back = (c - m) * rh * alpha;
-    const A fwd = (p - c) * rh * alpha;
-    if (!(central * fwd > A(0) && back * fwd > A(0))) return 0;
-    const A ac = fabs(central), ab = fabs(back), af = fabs(fwd);
-    const A inner = (af < ab) ? af : ab;
-    if (!(inner < ac)) return 1;
-    return (af < ab) ? 3 : 2;
+    const A d1 = c - m, d2 = p - c, dc = p - m;
+    if (!(dc * d2 > A(0) && d1 * d2 > A(0))) return 0;
+    const A a1 = fabs(d1), a2 = fabs(d2);
+    const A inner = (rh * alpha) * ((a2 < a1) ? a2 : a1);
+    if (!(inner < fabs(dc) * (rh * A(0.5)))) return 1;
+    return (a2 < a1) ? 3 : 2;
 }
 
 // Adds the adjoint of one slope component (sbar) to its three cells.
@@ -98,10 +96,10 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
     const A one = A(1), half = A(0.5), zero = A(0), two = A(2), onehalf = A(1.5);
     const A g = K.g, igm1 = K.igm1, kappa = K.kappa, hk = K.k * half, hh = K.h * half;
     // ---- forward: face states ----
-    const A rho_l = UL.rho + sL.rho * K.h * half, pi_l = UL.p + sL.p * K.h * half;
-    const A u_l = UL.un + sL.un * K.h * half, v_l = UL.ut + sL.ut * K.h * half;
-    const A rho_r = UR.rho - sR.rho * K.h * half, pi_r = UR.p - sR.p * K.h * half;
-    const A u_r = UR.un - sR.un * K.h * half, v_r = UR.ut - sR.ut * K.h * half;
+    const A rho_l = fma(sL.rho, hh, UL.rho), pi_l = fma(sL.p, hh, UL.p);
+    const A u_l = fma(sL.un, hh, UL.un), v_l = fma(sL.ut, hh, UL.ut);
+    const A rho_r = fma(-sR.rho, hh, UR.rho), pi_r = fma(-sR.p, hh, UR.p);
+    const A u_r = fma(-sR.un, hh, UR.un), v_r = fma(-sR.ut, hh, UR.ut);
     const A rho_lx = sL.rho, pi_lx = sL.p, u_lx = sL.un, v_lx = sL.ut;
     const A rho_rx = sR.rho, pi_rx = sR.p, u_rx = sR.un, v_rx = sR.ut;
     // ---- forward: Hoisted::grp ----

@@ -252,7 +252,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
     const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
     Cell<Real> A;
     if (FINAL) A = load_cell(a.comb, min(c, nx - 1), y, 2, 3);  // branch A, loaded early
-    const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);           // slope of cell c
+    const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);          // slope of cell c
     const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
     Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
     if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
@@ -319,11 +319,11 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
     const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
     auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
     Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
-    Cell<Real> sm1 = cell_slope(ld(l0 - 2), cm1, c0, K);
+    Cell<Real> sm1 = Phys::slope(ld(l0 - 2), cm1, c0, K);
     Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
     for (int l = l0; l <= lend; ++l) {
         const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
-        const Cell<Real> s0 = cell_slope(cm1, c0, cp1, K);
+        const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
         const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
         if (TAPE && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);  // interface l-1/2 at line position l
         if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
