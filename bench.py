@@ -442,18 +442,24 @@ def form_adjoint(args):
     t1 = time.perf_counter()
     grad = h.vjp(cot)[..., 0]
     t2 = time.perf_counter()
-    # device-timed: forward with checkpoints + reverse, through CUDA events around both calls
+    # device-timed: forward with checkpoints + reverse, through CUDA events
+    # around both calls; the best of three, as for the forward
     import torch
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    h.set_state(U)
-    torch.cuda.synchronize()
-    e0.record()
-    h.forward(steps, ck)
-    e1.record()
-    h.vjp(cot)
-    e2.record()
-    torch.cuda.synchronize()
-    ck_ms, vjp_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    best = None
+    for _ in range(3):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        h.set_state(U)
+        torch.cuda.synchronize()
+        e0.record()
+        h.forward(steps, ck)
+        e1.record()
+        h.vjp(cot)
+        e2.record()
+        torch.cuda.synchronize()
+        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
+        if best is None or sum(t) < sum(best):
+            best = t
+    ck_ms, vjp_ms = best
 
     def J(U0):
         return math.fsum(((run(U0)[0][..., 0] - target) ** 2).ravel())
