@@ -1,6 +1,6 @@
 // fvm2d_adjoint_math.cuh -- reverse-mode (adjoint) versions of the per-cell
-// and per-interface arithmetic of one sweep, for the FP64 build with shared
-// reciprocals (Hoisted in fvm2d_math.cuh).  Each function recomputes the
+// and per-interface arithmetic of one sweep, for the builds with shared
+// reciprocals (Hoisted in fvm2d_math.cuh), in the arithmetic type FVM2D_REAL.  Each function recomputes the
 // forward values it needs and then applies the transposed Jacobian of the
 // forward statements in reverse order.  Branches (limiter selection, wave
 // cases, max(0, .)) follow the forward values, so the derivative is the one
@@ -13,7 +13,7 @@
 namespace fvm2d {
 namespace FVM2D_VARIANT {
 
-using A = double;
+using A = FVM2D_REAL;
 
 struct Cell5 {
     A rho, p, un, ut, e;

@@ -128,11 +128,12 @@ struct fvm2d_solver {
     std::string record_dir = ".";
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
-    double *ckpt = nullptr;       // checkpoints of fvm2d_forward
-    double *tape = nullptr;       // one segment's steps, recomputed by fvm2d_vjp: per step its input
+    char *ckpt = nullptr;         // checkpoints of fvm2d_forward (states of the build's type)
+    char *tape = nullptr;         // one segment's steps, recomputed by fvm2d_vjp: per step its input
                                   // state, X(U), Y(U) and the fluxes of its four sweeps
-    double *adj = nullptr;        // adjoint work: 2 adjoints, 3 work states, the saved final state
-    int ck_count = 0, ck_len = 0, ck_cap = 0, seg_cap = 0, fwd_steps = -1;
+    char *adj = nullptr;          // adjoint work: 2 adjoints, 3 work states, the saved final state
+    size_t ck_bytes = 0, tape_bytes = 0, adj_bytes = 0;
+    int ck_count = 0, ck_len = 0, fwd_steps = -1, fwd_precision = -1;
     // fvm2d_vjp's graphs for a full segment: its taped recompute, and its
     // reverse starting from either adjoint buffer; built for vjp_len steps
     cudaGraphExec_t vjp_graph[3] = {nullptr, nullptr, nullptr};
@@ -888,26 +889,57 @@ int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt)
 static int diff_ready(fvm2d_solver *s)
 {
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
-    if (s->precision != FVM2D_FP64) return fail(FVM2D_ERR_INVALID, "differentiation runs on the FP64 build (FVM2D_FP64)");
+    if (s->precision != FVM2D_FP64 && s->precision != FVM2D_FP32)
+        return fail(FVM2D_ERR_INVALID, "differentiation runs on the FVM2D_FP64 or FVM2D_FP32 build");
     if (!(s->fixed_dt > 0.0)) return fail(FVM2D_ERR_INVALID, "set a fixed step size first (fvm2d_set_fixed_dt)");
     return FVM2D_OK;
 }
 
-// Copies host or device cells (stride doubles) into 4 double planes at dst,
-// staging through the sweep buffers.
-static int cells_to_planes(fvm2d_solver *s, const double *cells, int stride, double *dst)
+// Bytes of one state of the current build (4 planes of `plane` values).
+static size_t state_bytes_of(const fvm2d_solver *s)
+{
+    return (size_t)4 * s->plane * (is_fp32(s->precision) ? sizeof(float) : sizeof(double));
+}
+
+// (Re)allocates *buf to at least `bytes`; `grew` tells whether it moved.
+static int ensure(char *&buf, size_t &cap, size_t bytes, bool &grew)
+{
+    grew = false;
+    if (bytes <= cap) return FVM2D_OK;
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    cap = 0;
+    CK(cudaMalloc(&buf, bytes));
+    cap = bytes;
+    grew = true;
+    return FVM2D_OK;
+}
+
+// Copies host or device cells (stride doubles) into 4 planes at dst, of the
+// current build's type, staging through the sweep buffers.
+static int cells_to_planes(fvm2d_solver *s, const double *cells, int stride, void *dst)
 {
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
-    aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, dst, s->nx, s->ny, s->pitch, s->plane);
+    if (is_fp32(s->precision))
+        aos_to_soa<float><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, static_cast<float *>(dst), s->nx, s->ny,
+                                                          s->pitch, s->plane);
+    else
+        aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, static_cast<double *>(dst), s->nx,
+                                                           s->ny, s->pitch, s->plane);
     CK(cudaGetLastError());
     return FVM2D_OK;
 }
 
-static int planes_to_cells(fvm2d_solver *s, const double *src, double *cells, int stride)
+static int planes_to_cells(fvm2d_solver *s, const void *src, double *cells, int stride)
 {
-    soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(src, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    if (is_fp32(s->precision))
+        soa_to_aos<float><<<148 * 4, 256, 0, s->stream>>>(static_cast<const float *>(src), s->nx, s->ny, s->pitch,
+                                                          s->plane, stride, s->scratch);
+    else
+        soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(static_cast<const double *>(src), s->nx, s->ny, s->pitch,
+                                                           s->plane, stride, s->scratch);
     CK(cudaGetLastError());
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -919,6 +951,7 @@ int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tan
 {
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
+    if (s->precision != FVM2D_FP64) return fail(FVM2D_ERR_INVALID, "fvm2d_jvp runs on the FP64 build (FVM2D_FP64)");
     if (!tangent_in || !tangent_out) return fail(FVM2D_ERR_INVALID, "null tangent pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
     if (nsteps < 0) return fail(FVM2D_ERR_INVALID, "nsteps must be non-negative");
@@ -960,28 +993,23 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     if (checkpoints > nsteps) checkpoints = nsteps;
     const int len = (nsteps + checkpoints - 1) / checkpoints;
     const int count = (nsteps + len - 1) / len;
-    const long long n4 = 4 * s->plane;
-    if (count > s->ck_cap) {
-        if (s->ckpt) cudaFree(s->ckpt);
-        s->ckpt = nullptr;
-        s->ck_cap = 0;
-        CK(cudaMalloc(&s->ckpt, (size_t)count * n4 * sizeof(double)));
-        s->ck_cap = count;
-    }
-    if (int rc = s->build_graphs()) return rc;  // the step graphs of the fixed-dt FP64 build
+    const size_t sb = state_bytes_of(s);
+    bool grew;
+    if (int rc = ensure(s->ckpt, s->ck_bytes, (size_t)count * sb, grew)) return rc;
+    if (int rc = s->build_graphs()) return rc;  // the step graphs of the fixed-dt build
     StepControl *h = s->ctl_h;
     h->step_limit = INT_MAX;
     h->done = 0;
     h->active = 0;
     if (int rc = s->upload_control()) return rc;
     const LaunchConfig c = s->config();
-    CK(s->need_init ? kVariants[FVM2D_FP64].init(c, s->stream) : kVariants[FVM2D_FP64].plan(c, s->stream));
+    CK(s->need_init ? kVariants[s->precision].init(c, s->stream) : kVariants[s->precision].plan(c, s->stream));
     s->need_init = false;
     s->ck_t.assign(count, 0.0);
     double t = h->t;
     for (int k = 0; k < count; ++k) {
         s->ck_t[k] = t;
-        CK(cudaMemcpyAsync(s->ckpt + k * n4, s->U, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaMemcpyAsync(s->ckpt + k * sb, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
         const int m = (k + 1) * len <= nsteps ? len : nsteps - k * len;
         for (int j = 0; j < m;) {
             const int which = m - j >= fvm2d_solver::kGraphSteps[0] ? 0 : 1;
@@ -995,6 +1023,7 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     s->ck_count = count;
     s->ck_len = len;
     s->fwd_steps = nsteps;
+    s->fwd_precision = s->precision;
     s->total_steps += nsteps;
     return FVM2D_OK;
 }
@@ -1003,26 +1032,20 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
 {
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
-    if (s->fwd_steps < 0) return fail(FVM2D_ERR_STATE, "fvm2d_vjp reverses the last fvm2d_forward: call it first");
+    if (s->fwd_steps < 0 || s->fwd_precision != s->precision)
+        return fail(FVM2D_ERR_STATE, "fvm2d_vjp reverses the last fvm2d_forward of this build: call it first");
     if (!cotangent_in || !cotangent_out) return fail(FVM2D_ERR_INVALID, "null cotangent pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
-    const long long n4 = 4 * s->plane;
-    const size_t sb = n4 * sizeof(double);
+    const bool f32 = is_fp32(s->precision);
+    const size_t sb = state_bytes_of(s);
     constexpr int kTapeStates = 7;  // per step: U, X(U), Y(U), the fluxes of its 4 sweeps
-    if (s->ck_len > s->seg_cap) {
-        s->drop_vjp_graphs();
-        if (s->tape) cudaFree(s->tape);
-        s->tape = nullptr;
-        s->seg_cap = 0;
-        CK(cudaMalloc(&s->tape, (size_t)s->ck_len * kTapeStates * sb));
-        s->seg_cap = s->ck_len;
-    }
-    constexpr int kAdjStates = 6;  // two adjoints, three work states, the saved final state
-    if (!s->adj) {
-        s->drop_vjp_graphs();
-        CK(cudaMalloc(&s->adj, kAdjStates * sb));
-    }
-    double *lam = s->adj, *lam2 = s->adj + n4, *saved = s->adj + 5 * n4;
+    constexpr int kAdjStates = 6;   // two adjoints, three work states, the saved final state
+    bool grew_tape, grew_adj;
+    if (int rc = ensure(s->tape, s->tape_bytes, (size_t)s->ck_len * kTapeStates * sb, grew_tape)) return rc;
+    if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
+    if (grew_tape || grew_adj) s->drop_vjp_graphs();
+    char *const adj0 = s->adj, *const adj1 = s->adj + sb, *const saved = s->adj + 5 * sb;
+    char *lam = adj0, *lam2 = adj1;
     fvm2d::AdjointLaunch L;
     L.nx = s->nx;
     L.ny = s->ny;
@@ -1037,12 +1060,14 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     L.alpha = s->alpha;
     L.gamma = s->gamma;
     L.dt = s->fixed_dt;
-    for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * n4;
+    for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * sb;
     const StepControl after = *s->ctl_h;
     CK(cudaMemcpyAsync(saved, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
     if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
     StepControl *h = s->ctl_h;
-    auto tape = [&](int j, int q) { return s->tape + ((long long)j * kTapeStates + q) * n4; };
+    auto tape = [&](int j, int q) { return s->tape + ((size_t)j * kTapeStates + q) * sb; };
+    auto taped_step = f32 ? fvm2d::fp32::enqueue_step_taped : fvm2d::fp64::enqueue_step_taped;
+    auto adjoint_step = f32 ? fvm2d::adj32::adjoint_step : fvm2d::adj::adjoint_step;
     // the taped recompute of m steps from the state in U, and the reverse of
     // m steps from adjoint buffer `from` (the result lands in `from` for even m)
     auto recompute = [&](int m) -> int {
@@ -1052,13 +1077,12 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
             cj.A = tape(j, 1);
             cj.B = tape(j, 2);
             void *const flux[4] = {tape(j, 3), tape(j, 4), tape(j, 5), tape(j, 6)};
-            CK(fvm2d::fp64::enqueue_step_taped(cj, s->stream, flux));
+            CK(taped_step(cj, s->stream, flux));
         }
         return FVM2D_OK;
     };
-    double *const adj0 = s->adj, *const adj1 = s->adj + n4;
-    auto reverse = [&](int m, double *from) -> int {
-        double *a = from, *b = from == adj0 ? adj1 : adj0;
+    auto reverse = [&](int m, char *from) -> int {
+        char *a = from, *b = from == adj0 ? adj1 : adj0;
         for (int j = m - 1; j >= 0; --j) {
             L.U = tape(j, 0);
             L.A1 = tape(j, 1);
@@ -1066,16 +1090,16 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
             for (int q = 0; q < 4; ++q) L.flux[q] = tape(j, 3 + q);
             L.lb_out = a;
             L.lb_in = b;
-            CK(fvm2d::adjoint_step(L, s->stream));
+            CK(adjoint_step(L, s->stream));
             std::swap(a, b);
         }
         return FVM2D_OK;
     };
-    // graphs of a full segment, kept while the handle's parameters and
+    // graphs of a full segment, kept while the handle's parameters, build and
     // buffers stay the same
     if (s->vjp_len != s->ck_len && s->ck_count > 1) {
         s->drop_vjp_graphs();
-        CK(fvm2d::adjoint_prepare());
+        CK(f32 ? fvm2d::adj32::adjoint_prepare() : fvm2d::adj::adjoint_prepare());
         const int len = s->ck_len;
         if (int rc = s->capture(&s->vjp_graph[0], [&] { return recompute(len); })) return rc;
         if (int rc = s->capture(&s->vjp_graph[1], [&] { return reverse(len, adj0); })) return rc;
@@ -1085,14 +1109,13 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     for (int k = s->ck_count - 1; k >= 0; --k) {
         const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
         // recompute the segment from its checkpoint, taping every step
-        CK(cudaMemcpyAsync(s->U, s->ckpt + k * n4, sb, cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaMemcpyAsync(s->U, s->ckpt + k * sb, sb, cudaMemcpyDeviceToDevice, s->stream));
         std::memset(h, 0, sizeof(StepControl));
         h->t = s->ck_t[k];
         h->step_limit = INT_MAX;
         if (int rc = s->upload_control()) return rc;
-        CK(kVariants[FVM2D_FP64].plan(c, s->stream));
-        const bool full = m == s->vjp_len;
-        if (full) {
+        CK(kVariants[s->precision].plan(c, s->stream));
+        if (m == s->vjp_len) {
             CK(cudaGraphLaunch(s->vjp_graph[0], s->stream));
             CK(cudaGraphLaunch(s->vjp_graph[lam == adj0 ? 1 : 2], s->stream));
         } else {

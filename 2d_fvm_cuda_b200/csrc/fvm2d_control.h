@@ -66,11 +66,14 @@ FVM2D_DECLARE_VARIANT(fp64_reforder)
 FVM2D_DECLARE_VARIANT(fp32)
 FVM2D_DECLARE_VARIANT(jvp)
 
+// The FP64 and FP32 steps keeping what their adjoint needs: X(U) in c.A, Y(U)
+// in c.B and the interface fluxes of the four sweeps (X of U, Y of U, Y of A,
+// X of B), each stored at the interface's right cell in planes mass, normal
+// momentum, energy, tangential momentum.
 namespace fp64 {
-// The FP64 step keeping what its adjoint needs: X(U) in c.A, Y(U) in c.B and
-// the interface fluxes of its four sweeps (X of U, Y of U, Y of A, X of B),
-// each stored at the interface's right cell in planes mass, normal momentum,
-// energy, tangential momentum.
+cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4]);
+}
+namespace fp32 {
 cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4]);
 }
 

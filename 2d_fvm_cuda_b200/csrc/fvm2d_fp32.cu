@@ -8,6 +8,7 @@
 #define FVM2D_VARIANT fp32
 #define FVM2D_REAL float
 #define FVM2D_PHYS PackedCompensated
+#define FVM2D_TAPED_STEP  // also the taped step of FP32 differentiation runs
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to
 #ifdef FVM2D_TUNE_X

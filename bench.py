@@ -461,6 +461,35 @@ def form_adjoint(args):
             best = t
     ck_ms, vjp_ms = best
 
+    # the FP32 build on the same run: its cost and its gradient against FP64's
+    hf = pkg.Handle(n, n)
+    hf.configure(w, hgt, 1e9, 0.45, 1.9, 1.4, 5, pkg.FP32)
+    hf.set_fixed_dt(dt)
+    f32_fwd = []
+    for _ in range(3):
+        hf.set_state(U)
+        hf.advance(steps)
+        f32_fwd.append(hf.run_stats()[0])
+    best32, grad32 = None, None
+    for _ in range(3):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        hf.set_state(U)
+        torch.cuda.synchronize()
+        e0.record()
+        hf.forward(steps, ck)
+        e1.record()
+        grad32 = hf.vjp(cot)[..., 0]
+        e2.record()
+        torch.cuda.synchronize()
+        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
+        if best32 is None or sum(t) < sum(best32):
+            best32 = t
+    hf.close()
+    fp32 = {"forward_ms": min(f32_fwd), "forward_with_checkpoints_ms": best32[0], "vjp_ms": best32[1],
+            "forward_plus_adjoint_over_forward": sum(best32) / min(f32_fwd),
+            "gradient_rel_l2_vs_fp64": float(np.linalg.norm(grad32 - grad) / np.linalg.norm(grad)),
+            "cotangent": "the FP64 run's"}
+
     def J(U0):
         return math.fsum(((run(U0)[0][..., 0] - target) ** 2).ravel())
 
@@ -477,6 +506,7 @@ def form_adjoint(args):
             "forward_plus_adjoint_over_forward": (ck_ms + vjp_ms) / fwd_ms,
             "fd_check": {"direction": "6 smooth density modes", "eps": eps, "fd": fd, "adjoint": ad,
                          "rel_diff": abs(fd - ad) / abs(ad)},
+            "fp32": fp32,
             "wall_s": {"forward": t1 - t0, "vjp": t2 - t1}}
 
 

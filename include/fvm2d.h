@@ -218,8 +218,9 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
 
 /* ---- differentiation (no reference counterpart) ----------------------------
- * Derivatives of the FP64 step (FVM2D_FP64) with respect to the state, at a
- * fixed step size so the CFL maximum is not differentiated.  Branches of the
+ * Derivatives of the step with respect to the state, at a fixed step size so
+ * the CFL maximum is not differentiated: fvm2d_forward / fvm2d_vjp on the
+ * FVM2D_FP64 or FVM2D_FP32 build, fvm2d_jvp on FVM2D_FP64.  Branches of the
  * limiter and of the Riemann solver contribute the derivative of the branch
  * taken (almost everywhere). */
 
