@@ -273,7 +273,7 @@ class Handle:
     def set_rows_ptr(self, j0: int, nrows: int, ptr: int) -> None:
         check(self.lib.fvm2d_set_rows(self.h, int(j0), int(nrows), ptr))
 
-    # -- differentiation (fixed dt, FP64 build) --
+    # -- differentiation (fixed dt; forward/vjp on FP64 or FP32, jvp on FP64) --
     def set_fixed_dt(self, dt: float) -> None:
         check(self.lib.fvm2d_set_fixed_dt(self.h, float(dt)))
 
