@@ -366,16 +366,10 @@ def reference_arm(args, rank, world):
 # ---------------------------------------------------------------------------
 # The north star's other forms, each printed as its own JSON line.
 # ---------------------------------------------------------------------------
-def form_batch(args):
-    """Batched form: 256 seeded four-quadrant problems, per-side size from
-    {128, 192, ..., 1024}, split point ~U[0.3, 0.7]^2, t_end 0.2, each with its
-    own CFL dt; one launch per stage over all problems (graph-captured loop)
-    against 256 sequential solves with the same build."""
-    pkg = importlib.import_module("2d_fvm_cuda_b200")
+def _batch_case(pkg, spec, precisions, label):
     sc = pkg.scenarios
-    spec = sc.uneven_batch(256, 3)
-    out = {"form": "batch", "workload": "256 four-quadrant problems, sides 128..1024, t_end 0.2", "results": []}
-    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32")):
+    out = []
+    for prec, name in precisions:
         b = pkg.Batch([(n, m) for n, m, _, _ in spec])
         b.set_precision(prec)
         for p, (n, m, seed, split) in enumerate(spec):
@@ -397,12 +391,29 @@ def form_batch(args):
             h.close()
             worst = max(worst, max(float(np.nansum(np.abs(finals[p][..., f] - V[..., f])) /
                                          np.nansum(np.abs(V[..., f]))) for f in range(4)))
-        out["results"].append({"precision": name, "cell_updates": cu, "batch_s": bms / 1e3,
-                               "batch_cell_updates_per_s": cu / (bms / 1e3), "sequential_s": seq_ms / 1e3,
-                               "sequential_cell_updates_per_s": cu / (seq_ms / 1e3), "speedup": seq_ms / bms,
-                               "autotuned": {"y_segment_interfaces": T, "grid_blocks": g},
-                               "max_rel_l1_vs_sequential": worst, "gpu_launches": launches})
+        out.append({"workload": label, "precision": name, "cell_updates": cu, "batch_s": bms / 1e3,
+                    "batch_cell_updates_per_s": cu / (bms / 1e3), "sequential_s": seq_ms / 1e3,
+                    "sequential_cell_updates_per_s": cu / (seq_ms / 1e3), "speedup": seq_ms / bms,
+                    "autotuned": {"y_segment_interfaces": T, "grid_blocks": g},
+                    "max_rel_l1_vs_sequential": worst, "gpu_launches": launches})
     return out
+
+
+def form_batch(args):
+    """Batched form: 256 seeded four-quadrant problems, per-side size from
+    {128, 192, ..., 1024}, split point ~U[0.3, 0.7]^2, t_end 0.2, each with its
+    own CFL dt; one launch per stage over all problems (graph-captured loop)
+    against 256 sequential solves with the same build.  Beside it, an ensemble
+    of 1024 small problems (sides 32..128), where per-solve launch overheads
+    dominate and batching pays most."""
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    sc = pkg.scenarios
+    both = ((pkg.FP64, "fp64"), (pkg.FP32, "fp32"))
+    results = _batch_case(pkg, sc.uneven_batch(256, 3), both, "256 problems, sides 128..1024")
+    results += _batch_case(pkg, sc.uneven_batch(1024, 5, sizes=tuple(range(32, 129, 16))), both[:1],
+                           "1024 problems, sides 32..128")
+    return {"form": "batch", "workload": "four-quadrant problems, t_end 0.2, each with its own dt",
+            "results": results}
 
 
 def form_adjoint(args):
