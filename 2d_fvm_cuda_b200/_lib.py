@@ -41,6 +41,7 @@ SIGNATURES = [
     ("fvm2d_get_state", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     ("fvm2d_solve", ctypes.c_int, [_vp]),
     ("fvm2d_advance", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_get_health", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_set_record_model", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
     ("fvm2d_write_frame_png", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("fvm2d_write_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
@@ -222,6 +223,13 @@ class Handle:
         k = ctypes.c_int(0)
         check(self.lib.fvm2d_profile_kernels(self.h, int(nsteps), out, ctypes.byref(k)))
         return list(out), k.value
+
+    def first_bad_step(self) -> int:
+        """1-based step that first left a NaN or non-positive density or
+        pressure in an interior cell since the state was set; 0: none."""
+        k = ctypes.c_int(0)
+        check(self.lib.fvm2d_get_health(self.h, ctypes.byref(k)))
+        return k.value
 
     # -- frames and state files --
     def set_record_model(self, on: bool, gap_per_frame: int = 10, record_dir: str = ".") -> None:

@@ -92,10 +92,15 @@ __global__ void __launch_bounds__(NT, MINB) batch_sweep_x_kernel(BatchArgs<Real>
     long long pend = 0;
     bool active = false;
     double vmax = 0.0;
+    int bad = 0;
     for (; it < end; ++it) {
         if (it >= pend) {
-            if (FINAL && active) warp_max_to(vmax, &b.ctl[p].smax_bits);
+            if (FINAL && active) {
+                note_bad_cells(bad, b.ctl + p);
+                warp_max_to(vmax, &b.ctl[p].smax_bits);
+            }
             vmax = 0.0;
+            bad = 0;
             p = find_problem(b.x0, b.np, it);
             pend = b.x0[p + 1];
             active = b.ctl[p].active != 0;
@@ -110,9 +115,12 @@ __global__ void __launch_bounds__(NT, MINB) batch_sweep_x_kernel(BatchArgs<Real>
         const SweepConsts<Real> K = sweep_consts(a, b.ctl[p].dt);
         const int nseg = b.prob[p].nsegx;
         const long long local = it - b.x0[p];
-        x_item<Real, Phys, FINAL>(a, K, int(local / nseg), int(local % nseg), nseg, lane, vmax);
+        x_item<Real, Phys, FINAL>(a, K, int(local / nseg), int(local % nseg), nseg, lane, vmax, bad);
     }
-    if (FINAL && active) warp_max_to(vmax, &b.ctl[p].smax_bits);
+    if (FINAL && active) {
+        note_bad_cells(bad, b.ctl + p);
+        warp_max_to(vmax, &b.ctl[p].smax_bits);
+    }
 }
 
 template <typename Real, class Phys, int NT, int MINB>

@@ -39,6 +39,9 @@ int fail(int code, const std::string &msg) { return fvm2d::report_error(code, ms
 
 int cuda_fail(cudaError_t e, const char *what)
 {
+    // clear a pending error that is not sticky (a failed allocation, say), so
+    // that it is not reported again by the next call's launch checks
+    cudaGetLastError();
     return fail(FVM2D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 

@@ -48,6 +48,9 @@ int fail(int code, const std::string &msg)
 
 int cuda_fail(cudaError_t e, const char *what)
 {
+    // clear a pending error that is not sticky (a failed allocation, say), so
+    // that it is not reported again by the next call's launch checks
+    cudaGetLastError();
     return fail(FVM2D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -797,6 +800,14 @@ int fvm2d_read_state(fvm2d_solver *s, const char *path)
     if (int rc = fvm2d_set_state(s, cells.data(), 4)) return rc;
     s->ctl_h->t = hd.t;  // fvm2d_advance continues from the saved time and step count
     s->ctl_h->steps = int(hd.steps);
+    return FVM2D_OK;
+}
+
+int fvm2d_get_health(fvm2d_solver *s, int *first_bad_step)
+{
+    if (int rc = check(s)) return rc;
+    if (!first_bad_step) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    *first_bad_step = s->ctl_h->first_bad;
     return FVM2D_OK;
 }
 

@@ -18,7 +18,8 @@ struct StepControl {
     int active;                    // 1 while a step is in flight
     int done;                      // 1 once the loop of wrappers.cuh:196 has ended
     unsigned int ticket;           // last-block detection in grid reductions
-    int pad;
+    int first_bad;                 // 1-based step that first left an interior cell with NaN or
+                                   // non-positive density or pressure; 0: none
 };
 
 struct PlanParams {

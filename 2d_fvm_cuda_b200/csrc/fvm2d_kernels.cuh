@@ -85,6 +85,13 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long *bits)
     }
 }
 
+// Records the step in flight as the first to leave a bad cell, if any lane of
+// the warp saw one and no earlier step did.  Called by all lanes of a warp.
+__device__ __forceinline__ void note_bad_cells(int bad, StepControl *ctl)
+{
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicCAS(&ctl->first_bad, 0, ctl->steps + 1);
+}
+
 // True in exactly one thread of the last block of the grid to get here, after
 // every earlier block's global writes are visible.
 __device__ __forceinline__ bool last_block_done(unsigned int *ticket)
@@ -239,11 +246,12 @@ __device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
 constexpr int kXCells = 30;
 
 // One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
-// wave speed of the interior cells written by a final sweep; a TAPE sweep
+// wave speed of the interior cells written by a final sweep, and bad whether
+// one of them holds NaN or a non-positive density or pressure; a TAPE sweep
 // also stores every interface flux it computes.
 template <typename Real, class Phys, bool FINAL, bool TAPE = false>
 __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int y, int seg,
-                                       int nseg, int lane, double &vmax)
+                                       int nseg, int lane, double &vmax, int &bad)
 {
     const int nx = a.nx, ny = a.ny;
     const int c = 1 + seg * kXCells + lane;
@@ -266,8 +274,10 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
             o.un = (Ab.un + U.un) * Real(0.5);
             o.ut = (Ab.ut + U.ut) * Real(0.5);
             store_cell(a.dst, x, y, 2, 3, o);
-            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3)
+            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3) {
                 vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
+                bad |= !(o.rho > Real(0) && o.p > Real(0));  // NaN fails both tests
+            }
         } else {
             store_cell(a.dst, x, y, 2, 3, U);
         }
@@ -297,9 +307,13 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     const long long nwork = (long long)nseg * a.ny;
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
+    int bad = 0;
     for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
-        x_item<Real, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax);
-    if (FINAL) block_max_to<NT>(vmax, &a.ctl->smax_bits);
+        x_item<Real, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax, bad);
+    if (FINAL) {
+        note_bad_cells(bad, a.ctl);
+        block_max_to<NT>(vmax, &a.ctl->smax_bits);
+    }
 }
 
 // Segments of T interfaces (T-1 updated cells) along a y line of ny cells.

@@ -43,6 +43,9 @@ int fail(int code, const std::string &msg) { return fvm2d::report_error(code, ms
 
 int cuda_fail(cudaError_t e, const char *what)
 {
+    // clear a pending error that is not sticky (a failed allocation, say), so
+    // that it is not reported again by the next call's launch checks
+    cudaGetLastError();
     return fail(FVM2D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -59,7 +62,7 @@ __global__ void reset_control(fvm2d::StepControl *c, double t0, int nsteps)
     c->active = 0;
     c->done = 0;
     c->ticket = 0u;
-    c->pad = 0;
+    c->first_bad = 0;
 }
 
 // Once per device, with that device current: the device address of

@@ -143,6 +143,13 @@ int fvm2d_solve(fvm2d_solver *s);
  * benchmarks). */
 int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done);
 
+/* Health of the run (no reference counterpart: the reference checks
+ * nothing).  *first_bad_step receives the number, counted from 1 since the
+ * state was set, of the first step that left an interior cell with NaN or a
+ * non-positive density or pressure; 0 if none has.  The run goes on either
+ * way, as the reference's does. */
+int fvm2d_get_health(fvm2d_solver *s, int *first_bad_step);
+
 /* ---- frames and state files -----------------------------------------------
  * Frame recording replaces RGRP_2D_CUDA::setRecordModel / writeStagesTo_png
  * (src/wrappers.cuh:147-152, 253-260, 323-345): with recording on,

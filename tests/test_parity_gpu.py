@@ -244,3 +244,44 @@ def test_state_planes_from_host_and_device_memory(pkg, precision):
     assert np.array_equal(out.cpu().numpy(), np.moveaxis(a.get_state(4), -1, 0))
     for h in (a, b, c):
         h.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1, 3])
+def test_health_flags_the_first_bad_step(pkg, precision):
+    """Fault injection on the host: a corrupted input cell (negative pressure,
+    NaN density) must be reported as the first bad step; a clean run reports
+    none, and setting a clean state clears the record.  The run itself goes
+    on as the reference's does."""
+    n = 40
+    U = pkg.scenarios.seeded_four_quadrant(n, n, 17)
+    h = pkg.Handle(n, n)
+    h.configure(1.0, 1.0, 0.2, 0.45, 1.9, 1.4, 0, precision)
+    h.set_state(U)
+    h.advance(5)
+    assert h.first_bad_step() == 0
+    for field, value in ((1, -1.0), (0, float("nan"))):
+        B = U.copy()
+        B[20, 17, field] = value
+        h.set_state(B)
+        assert h.first_bad_step() == 0
+        h.advance(4)
+        assert h.first_bad_step() == 1, (field, h.first_bad_step())
+    h.set_state(U)
+    h.advance(3)
+    assert h.first_bad_step() == 0
+    h.close()
+
+
+def test_allocation_failure_is_reported_and_leaves_the_device_usable(pkg):
+    """Fault injection: a solver whose three state buffers (~200 GB at
+    46000^2) exceed the GPU's memory must fail with the library's CUDA error
+    and free what it had allocated; a normal solver works afterwards."""
+    with pytest.raises(pkg.FVM2DError) as e:
+        pkg.Handle(46000, 46000)
+    assert e.value.code == pkg._lib.FVM2D_ERR_CUDA
+    h = pkg.Handle(32, 32)
+    h.configure(1.0, 1.0, 0.01, 0.45, 1.9, 1.4, 0, 0)
+    h.set_state(pkg.scenarios.seeded_four_quadrant(32, 32, 1))
+    h.solve()
+    assert h.time()[0] == pytest.approx(0.01) and h.first_bad_step() == 0
+    h.close()
