@@ -9,7 +9,10 @@
 //   CUDA graphs of 16 steps and of 1 step (5 kernels each) replayed until
 //   the control record says the loop has ended, so the only host round trip
 //   is one 64-byte read per graph replay (the reference reads the max wave
-//   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284).
+//   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284);
+//   and, allocated on first use, the differentiation workspaces (dual-number
+//   states of fvm2d_jvp; checkpoints, one segment's tape and the adjoint
+//   states of fvm2d_forward / fvm2d_vjp, with graphs of a full segment).
 #include "../../include/fvm2d.h"
 #include "fvm2d_io.cuh"
 #include "fvm2d_adjoint.h"
