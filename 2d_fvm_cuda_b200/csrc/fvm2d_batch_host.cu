@@ -17,6 +17,7 @@
 // contraction-free build; in the builds with FMA contraction the two agree to
 // rounding (the compiler may contract the same inlined arithmetic differently
 // in the batched and the single-problem kernels).
+#include <nvtx3/nvToolsExt.h>
 #include "../../include/fvm2d.h"
 #include "fvm2d_batch_control.h"
 #include "fvm2d_transfer.cuh"
@@ -453,6 +454,8 @@ int fvm2d_batch_get_state(fvm2d_batch *b, int p, double *cells, int stride)
 
 int fvm2d_batch_solve(fvm2d_batch *b)
 {
+    nvtxRangePushA("fvm2d_batch_solve");
+    struct Pop { ~Pop() { nvtxRangePop(); } } pop_;
     if (int rc = check(b)) return rc;
     for (int p = 0; p < b->np; ++p)
         if (!b->have_state[p]) return fail(FVM2D_ERR_STATE, "every problem needs a state before solving");

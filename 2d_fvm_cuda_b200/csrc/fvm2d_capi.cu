@@ -20,6 +20,8 @@
 #include "fvm2d_dual.cuh"
 #include "fvm2d_transfer.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -62,6 +64,13 @@ int cuda_fail(cudaError_t e, const char *what)
         cudaError_t e_ = (call);                                              \
         if (e_ != cudaSuccess) return cuda_fail(e_, #call);                   \
     } while (0)
+
+// An NVTX range over a library call (visible in nsys / ncu; no cost without
+// a profiler attached).
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 struct Variant {
     cudaError_t (*prepare)();
@@ -444,6 +453,7 @@ int fvm2d_set_time_layout(fvm2d_solver *s, double end_time, double cfl)
 
 int fvm2d_set_state(fvm2d_solver *s, const double *cells, int stride)
 {
+    Range range_("fvm2d_set_state");
     if (int rc = check(s)) return rc;
     if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
@@ -498,6 +508,7 @@ int fvm2d_set_rp_initial_data(fvm2d_solver *s, const double *U1, const double *U
 
 int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride)
 {
+    Range range_("fvm2d_get_state");
     if (int rc = check(s)) return rc;
     if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
@@ -570,6 +581,7 @@ static int solve_recording(fvm2d_solver *s)
 
 int fvm2d_solve(fvm2d_solver *s)
 {
+    Range range_("fvm2d_solve");
     if (int rc = check(s)) return rc;
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
     StepControl *c = s->ctl_h;
@@ -593,6 +605,7 @@ int fvm2d_solve(fvm2d_solver *s)
 
 int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done)
 {
+    Range range_("fvm2d_advance");
     if (steps_done) *steps_done = 0;
     if (int rc = check(s)) return rc;
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
@@ -620,6 +633,7 @@ int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done)
 
 int fvm2d_advance_dt(fvm2d_solver *s, double dt)
 {
+    Range range_("fvm2d_advance_dt");
     if (int rc = check(s)) return rc;
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(FVM2D_ERR_INVALID, "dt must be positive and finite");
@@ -849,6 +863,7 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
 
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done)
 {
+    Range range_("fvm2d_profile_kernels");
     if (steps_done) *steps_done = 0;
     if (int rc = check(s)) return rc;
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
@@ -963,6 +978,7 @@ static int planes_to_cells(fvm2d_solver *s, const void *src, double *cells, int 
 
 int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tangent_out, int stride)
 {
+    Range range_("fvm2d_jvp");
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
     if (s->precision != FVM2D_FP64) return fail(FVM2D_ERR_INVALID, "fvm2d_jvp runs on the FP64 build (FVM2D_FP64)");
@@ -1001,6 +1017,7 @@ int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tan
 
 int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
 {
+    Range range_("fvm2d_forward");
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
     if (nsteps < 1 || checkpoints < 1) return fail(FVM2D_ERR_INVALID, "nsteps and checkpoints must be positive");
@@ -1044,6 +1061,7 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
 
 int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out, int stride)
 {
+    Range range_("fvm2d_vjp");
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
     if (s->fwd_steps < 0 || s->fwd_precision != s->precision)
