@@ -242,12 +242,14 @@ def product_arm(args, rank, world, local_rank):
     hf.advance(kp)
     F32 = hf.get_state(4)
     f32_l1 = [float(np.abs(F32[..., f] - A[..., f]).sum() / np.abs(A[..., f]).sum()) for f in range(4)]
+    f32_linf = [float(np.abs(F32[..., f] - A[..., f]).max()) for f in range(4)]
     hf.close()
     f32_ms = allreduce_max(dist, f32_ms)
     fp32 = {"value": n * n * args.steps * world / (f32_ms / 1e3), "unit": UNIT, "ms_per_step": f32_ms / args.steps,
             "speedup_vs_fp64": dev_ms_max / f32_ms,
             "l1_rel_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_l1,
                                "steps": args.warmup + 8 + args.steps + kp},
+            "linf_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_linf},
             "arithmetic": "FP32 planes and arithmetic, compensated update, FP64 wave-speed max and dt"}
 
     # e2e through the C ABI with pinned host buffers
