@@ -553,6 +553,7 @@ def form_vortex(args):
     res["fp64"]["rho_rel_l1_vs_exact"] = rl1(states["fp64"], E)
     res["fp32"]["rho_rel_l1_vs_exact"] = rl1(states["fp32"], E)
     res["fp32"]["rho_rel_l1_vs_fp64"] = rl1(states["fp32"], states["fp64"])
+    res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(states["fp32"][inner][..., 0] - states["fp64"][inner][..., 0]).max())
     res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
     return {"form": "vortex", "workload": "2000^2 periodic isentropic vortex, one period", "results": res}
 
