@@ -32,6 +32,10 @@ template <typename Real>
 __device__ __forceinline__ Real rmin(Real a, Real b) { return (b < a) ? b : a; }
 template <typename Real>
 __device__ __forceinline__ Real rmax(Real a, Real b) { return (a < b) ? b : a; }
+// single precision: the min/max instructions (equal to the selects unless an
+// argument is NaN)
+__device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 
 // Generalized-minmod slope of one component from its left (m), centre (c)
 // and right (p) values.  src/basicFuns.cuh:49-68.
@@ -282,6 +286,15 @@ __device__ __forceinline__ Real limited_slope_hoisted(Real m, Real c, Real p, Re
         return dc <= Real(0) ? -a : a;
     }
     return Real(0);
+}
+
+// Single precision: the same choices with the min/max and sign instructions
+// (they differ from the selects above only when an argument is NaN).
+__device__ __forceinline__ float limited_slope_hoisted(float m, float c, float p, float hrh, float rha)
+{
+    const float d1 = c - m, d2 = p - c, dc = p - m;
+    const float a = fminf(fabsf(dc) * hrh, rha * fminf(fabsf(d1), fabsf(d2)));
+    return fminf(dc * d2, d1 * d2) > 0.f ? copysignf(a, dc) : 0.f;
 }
 
 struct Hoisted {
