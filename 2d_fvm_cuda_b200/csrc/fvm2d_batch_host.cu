@@ -297,6 +297,8 @@ int fvm2d_batch_create(fvm2d_batch **out, int nproblems, const int *nx, const in
     for (int p = 0; p < nproblems; ++p) {
         if (nx[p] < 6 || ny[p] < 6) return fail(FVM2D_ERR_INVALID, "every nx and ny must be at least 6");
         if ((long long)nx[p] * ny[p] > (1ll << 31) - 1) return fail(FVM2D_ERR_INVALID, "nx * ny must stay below 2^31");
+        if ((long long)((nx[p] + 31) / 32 * 32) * ny[p] > (1ll << 31) - 1)
+            return fail(FVM2D_ERR_INVALID, "the padded plane, round_up(nx, 32) * ny, must stay below 2^31");
     }
     fvm2d_batch *b = new (std::nothrow) fvm2d_batch();
     if (!b) return fail(FVM2D_ERR_INVALID, "out of host memory");

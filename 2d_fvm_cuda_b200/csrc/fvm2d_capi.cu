@@ -339,6 +339,8 @@ int fvm2d_create(fvm2d_solver **out, int nx, int ny)
     *out = nullptr;
     if (nx < 6 || ny < 6) return fail(FVM2D_ERR_INVALID, "nx and ny must be at least 6 (two ghost layers per side)");
     if ((long long)nx * ny > (1ll << 31) - 1) return fail(FVM2D_ERR_INVALID, "nx * ny must stay below 2^31");
+    if ((long long)((nx + 31) / 32 * 32) * ny > (1ll << 31) - 1)
+        return fail(FVM2D_ERR_INVALID, "the padded plane, round_up(nx, 32) * ny, must stay below 2^31");
     fvm2d_solver *s = new (std::nothrow) fvm2d_solver();
     if (!s) return fail(FVM2D_ERR_INVALID, "out of host memory");
     cudaError_t e = cudaGetDevice(&s->device);
