@@ -71,8 +71,9 @@ const char *fvm2d_last_error(void);
 /* Library version string. */
 const char *fvm2d_version(void);
 
-/* Creates a solver for an nx x ny array (ghosts included, nx, ny >= 6) on
- * the current CUDA device.  Replaces RGRP_2D_CUDA(const vector<vector<vec5d>>&)
+/* Creates a solver for an nx x ny array (ghosts included, nx, ny >= 6, and
+ * nx rounded up to a multiple of 32 times ny below 2^31) on the current CUDA
+ * device.  Replaces RGRP_2D_CUDA(const vector<vector<vec5d>>&)
  * (src/wrappers.cuh:67-78) together with fvm2d_set_state, and the sizes of
  * setRPInitialData (src/wrappers.cuh:80-85).  Defaults as the reference
  * (src/wrappers.cuh:49-52): width = height = 1, end time 0, CFL 0.5,
