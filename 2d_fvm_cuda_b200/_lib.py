@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(PKG_DIR, "lib", "libfvm2d.so")
 
 FVM2D_OK, FVM2D_ERR_INVALID, FVM2D_ERR_CUDA, FVM2D_ERR_STATE = 0, 1, 2, 3
 FP64, FP64_STRICT, FP64_REFORDER, FP32 = 0, 1, 2, 3
+FULL_TAPE = 0  # fvm2d_forward(checkpoints=FULL_TAPE): tape every step, no recompute in vjp
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -293,6 +294,8 @@ class Handle:
         return out
 
     def forward(self, nsteps: int, checkpoints: int) -> None:
+        """nsteps steps keeping `checkpoints` states for vjp(), or with
+        checkpoints=FULL_TAPE the whole tape (7 states per step)."""
         check(self.lib.fvm2d_forward(self.h, int(nsteps), int(checkpoints)))
 
     def vjp(self, cotangent) -> np.ndarray:

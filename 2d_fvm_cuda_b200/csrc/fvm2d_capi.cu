@@ -144,11 +144,13 @@ struct fvm2d_solver {
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
     char *ckpt = nullptr;         // checkpoints of fvm2d_forward (states of the build's type)
-    char *tape = nullptr;         // one segment's steps, recomputed by fvm2d_vjp: per step its input
-                                  // state, X(U), Y(U) and the fluxes of its four sweeps
+    char *tape = nullptr;         // one segment's steps, recomputed by fvm2d_vjp (or every step, written
+                                  // by a full-tape fvm2d_forward): per step its input state, X(U), Y(U)
+                                  // and the fluxes of its four sweeps
     char *adj = nullptr;          // adjoint work: 2 adjoints, 3 work states, the saved final state
     size_t ck_bytes = 0, tape_bytes = 0, adj_bytes = 0;
     int ck_count = 0, ck_len = 0, fwd_steps = -1, fwd_precision = -1;
+    bool full_tape = false;       // the last fvm2d_forward kept every step's tape
     // fvm2d_vjp's graphs for a full segment: its taped recompute, and its
     // reverse starting from either adjoint buffer; built for vjp_len steps
     cudaGraphExec_t vjp_graph[3] = {nullptr, nullptr, nullptr};
@@ -197,6 +199,10 @@ struct fvm2d_solver {
         }
         graph_variant = -1;
         drop_vjp_graphs();
+        if (full_tape) {  // a parameter changed: the tape no longer belongs to this solver's step
+            full_tape = false;
+            fwd_steps = -1;
+        }
     }
 
     void drop_vjp_graphs()
@@ -1017,12 +1023,84 @@ int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tan
     return FVM2D_OK;
 }
 
+constexpr int kTapeStates = 7;  // per taped step: U, X(U), Y(U), the fluxes of its 4 sweeps
+
+// State q of taped step j.
+static char *tape_at(const fvm2d_solver *s, int j, int q, size_t sb)
+{
+    return s->tape + ((size_t)j * kTapeStates + q) * sb;
+}
+
+// Enqueues m taped steps (control planned) from the state in tape slot 0:
+// step j reads slot j's input state, fills the rest of slot j and writes its
+// result as slot j+1's input state, the last step's into U.
+static int taped_steps(fvm2d_solver *s, const LaunchConfig &c, int m)
+{
+    const size_t sb = state_bytes_of(s);
+    auto taped_step = is_fp32(s->precision) ? fvm2d::fp32::enqueue_step_taped : fvm2d::fp64::enqueue_step_taped;
+    for (int j = 0; j < m; ++j) {
+        LaunchConfig cj = c;
+        cj.U = tape_at(s, j, 0, sb);
+        cj.A = tape_at(s, j, 1, sb);
+        cj.B = tape_at(s, j, 2, sb);
+        void *const flux[4] = {tape_at(s, j, 3, sb), tape_at(s, j, 4, sb), tape_at(s, j, 5, sb),
+                               tape_at(s, j, 6, sb)};
+        void *const out = j + 1 < m ? static_cast<void *>(tape_at(s, j + 1, 0, sb)) : static_cast<void *>(s->U);
+        CK(taped_step(cj, s->stream, flux, out));
+    }
+    return FVM2D_OK;
+}
+
+// fvm2d_forward with FVM2D_FULL_TAPE: the forward steps are the taped ones.
+static int forward_full_tape(fvm2d_solver *s, int nsteps)
+{
+    const size_t sb = state_bytes_of(s);
+    const size_t need = (size_t)nsteps * kTapeStates * sb;
+    if (need > s->tape_bytes) {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        if (need > free_b + s->tape_bytes) {
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "the full tape needs %.2f GB, more than the device's free memory: use checkpoints",
+                          need / 1e9);
+            return fail(FVM2D_ERR_INVALID, msg);
+        }
+    }
+    s->full_tape = false;
+    s->fwd_steps = -1;
+    bool grew;
+    if (int rc = ensure(s->tape, s->tape_bytes, need, grew)) return rc;
+    if (grew) s->drop_vjp_graphs();
+    if (int rc = s->build_graphs()) return rc;  // as fvm2d_forward, so a later advance keeps the tape
+    StepControl *h = s->ctl_h;
+    h->step_limit = INT_MAX;
+    h->done = 0;
+    h->active = 0;
+    if (int rc = s->upload_control()) return rc;
+    const LaunchConfig c = s->config();
+    CK(s->need_init ? kVariants[s->precision].init(c, s->stream) : kVariants[s->precision].plan(c, s->stream));
+    s->need_init = false;
+    CK(cudaMemcpyAsync(tape_at(s, 0, 0, sb), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+    if (int rc = taped_steps(s, c, nsteps)) return rc;
+    CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->ck_count = 1;
+    s->ck_len = nsteps;
+    s->fwd_steps = nsteps;
+    s->fwd_precision = s->precision;
+    s->full_tape = true;
+    s->total_steps += nsteps;
+    return FVM2D_OK;
+}
+
 int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
 {
     Range range_("fvm2d_forward");
     if (int rc = check(s)) return rc;
     if (int rc = diff_ready(s)) return rc;
-    if (nsteps < 1 || checkpoints < 1) return fail(FVM2D_ERR_INVALID, "nsteps and checkpoints must be positive");
+    if (nsteps < 1 || checkpoints < 0)
+        return fail(FVM2D_ERR_INVALID, "nsteps must be positive and checkpoints positive or FVM2D_FULL_TAPE");
+    if (checkpoints == FVM2D_FULL_TAPE) return forward_full_tape(s, nsteps);
     if (checkpoints > nsteps) checkpoints = nsteps;
     const int len = (nsteps + checkpoints - 1) / checkpoints;
     const int count = (nsteps + len - 1) / len;
@@ -1057,6 +1135,7 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     s->ck_len = len;
     s->fwd_steps = nsteps;
     s->fwd_precision = s->precision;
+    s->full_tape = false;
     s->total_steps += nsteps;
     return FVM2D_OK;
 }
@@ -1072,8 +1151,7 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
     const bool f32 = is_fp32(s->precision);
     const size_t sb = state_bytes_of(s);
-    constexpr int kTapeStates = 7;  // per step: U, X(U), Y(U), the fluxes of its 4 sweeps
-    constexpr int kAdjStates = 6;   // two adjoints, three work states, the saved final state
+    constexpr int kAdjStates = 6;  // two adjoints, three work states, the saved final state
     bool grew_tape, grew_adj;
     if (int rc = ensure(s->tape, s->tape_bytes, (size_t)s->ck_len * kTapeStates * sb, grew_tape)) return rc;
     if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
@@ -1099,22 +1177,12 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     CK(cudaMemcpyAsync(saved, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
     if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
     StepControl *h = s->ctl_h;
-    auto tape = [&](int j, int q) { return s->tape + ((size_t)j * kTapeStates + q) * sb; };
-    auto taped_step = f32 ? fvm2d::fp32::enqueue_step_taped : fvm2d::fp64::enqueue_step_taped;
+    auto tape = [&](int j, int q) { return tape_at(s, j, q, sb); };
     auto adjoint_step = f32 ? fvm2d::adj32::adjoint_step : fvm2d::adj::adjoint_step;
-    // the taped recompute of m steps from the state in U, and the reverse of
-    // m steps from adjoint buffer `from` (the result lands in `from` for even m)
-    auto recompute = [&](int m) -> int {
-        for (int j = 0; j < m; ++j) {
-            CK(cudaMemcpyAsync(tape(j, 0), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-            LaunchConfig cj = c;
-            cj.A = tape(j, 1);
-            cj.B = tape(j, 2);
-            void *const flux[4] = {tape(j, 3), tape(j, 4), tape(j, 5), tape(j, 6)};
-            CK(taped_step(cj, s->stream, flux));
-        }
-        return FVM2D_OK;
-    };
+    // the taped recompute of m steps from the state in tape slot 0, and the
+    // reverse of m steps from adjoint buffer `from` (the result lands in
+    // `from` for even m)
+    auto recompute = [&](int m) -> int { return taped_steps(s, c, m); };
     auto reverse = [&](int m, char *from) -> int {
         char *a = from, *b = from == adj0 ? adj1 : adj0;
         for (int j = m - 1; j >= 0; --j) {
@@ -1131,7 +1199,7 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     };
     // graphs of a full segment, kept while the handle's parameters, build and
     // buffers stay the same
-    if (s->vjp_len != s->ck_len && s->ck_count > 1) {
+    if (!s->full_tape && s->vjp_len != s->ck_len && s->ck_count > 1) {
         s->drop_vjp_graphs();
         CK(f32 ? fvm2d::adj32::adjoint_prepare() : fvm2d::adj::adjoint_prepare());
         const int len = s->ck_len;
@@ -1142,8 +1210,13 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
     }
     for (int k = s->ck_count - 1; k >= 0; --k) {
         const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
+        if (s->full_tape) {  // the forward taped every step: reverse only
+            if (int rc = reverse(m, lam)) return rc;
+            if (m & 1) std::swap(lam, lam2);
+            continue;
+        }
         // recompute the segment from its checkpoint, taping every step
-        CK(cudaMemcpyAsync(s->U, s->ckpt + k * sb, sb, cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaMemcpyAsync(tape(0, 0), s->ckpt + k * sb, sb, cudaMemcpyDeviceToDevice, s->stream));
         std::memset(h, 0, sizeof(StepControl));
         h->t = s->ck_t[k];
         h->step_limit = INT_MAX;

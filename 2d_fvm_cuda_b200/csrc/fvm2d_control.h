@@ -70,12 +70,13 @@ FVM2D_DECLARE_VARIANT(jvp)
 // The FP64 and FP32 steps keeping what their adjoint needs: X(U) in c.A, Y(U)
 // in c.B and the interface fluxes of the four sweeps (X of U, Y of U, Y of A,
 // X of B), each stored at the interface's right cell in planes mass, normal
-// momentum, energy, tangential momentum.
+// momentum, energy, tangential momentum.  The step reads c.U and writes its
+// result to `out` (c.U when null).
 namespace fp64 {
-cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4]);
+cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4], void *out);
 }
 namespace fp32 {
-cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4]);
+cudaError_t enqueue_step_taped(const LaunchConfig &c, cudaStream_t s, void *const flux[4], void *out);
 }
 
 // Records `msg` as the calling thread's fvm2d_last_error() text; returns code.

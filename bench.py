@@ -422,7 +422,9 @@ def form_adjoint(args):
     """Differentiation form: 512^2 periodic [0,10]^2, isentropic vortex plus 16
     seeded density modes (amplitude <= 1e-3), fixed CFL-safe dt, 200 steps,
     J = sum (rho_T - rho_target)^2 with the target from a second seeded
-    perturbation, gradient by fvm2d_vjp with ceil(sqrt(200)) = 15 checkpoints."""
+    perturbation, gradient by fvm2d_vjp with ceil(sqrt(200)) = 15 checkpoints,
+    and again with the full tape (FVM2D_FULL_TAPE: every step taped by the
+    forward, nothing recomputed)."""
     import math
     pkg = importlib.import_module("2d_fvm_cuda_b200")
     sc = pkg.scenarios
@@ -455,24 +457,36 @@ def form_adjoint(args):
     t1 = time.perf_counter()
     grad = h.vjp(cot)[..., 0]
     t2 = time.perf_counter()
-    # device-timed: forward with checkpoints + reverse, through CUDA events
-    # around both calls; the best of three, as for the forward
+    # device-timed: forward with checkpoints (or the full tape) + reverse,
+    # through CUDA events around both calls; the best of three, as for the
+    # forward
     import torch
-    best = None
-    for _ in range(3):
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        h.set_state(U)
-        torch.cuda.synchronize()
-        e0.record()
-        h.forward(steps, ck)
-        e1.record()
-        h.vjp(cot)
-        e2.record()
-        torch.cuda.synchronize()
-        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
-        if best is None or sum(t) < sum(best):
-            best = t
-    ck_ms, vjp_ms = best
+
+    def timed(hd, checkpoints):
+        best, g = None, None
+        for _ in range(3):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            hd.set_state(U)
+            torch.cuda.synchronize()
+            e0.record()
+            hd.forward(steps, checkpoints)
+            e1.record()
+            g = hd.vjp(cot)[..., 0]
+            e2.record()
+            torch.cuda.synchronize()
+            t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
+            if best is None or sum(t) < sum(best):
+                best = t
+        return best, g
+
+    ck_ms, vjp_ms = timed(h, ck)[0]
+    # the whole tape kept instead of checkpoints: 7 states per step
+    # (200 x 7 x 8.4 MB = 11.7 GB in FP64), no recompute in the VJP
+    (tape_fwd_ms, tape_vjp_ms), grad_tape = timed(h, pkg.FULL_TAPE)
+    full_tape = {"forward_ms": tape_fwd_ms, "vjp_ms": tape_vjp_ms,
+                 "forward_plus_adjoint_over_forward": (tape_fwd_ms + tape_vjp_ms) / fwd_ms,
+                 "tape_gb": steps * 7 * 4 * n * n * 8 / 1e9,
+                 "gradient_rel_l2_vs_checkpoints": float(np.linalg.norm(grad_tape - grad) / np.linalg.norm(grad))}
 
     # the FP32 build on the same run: its cost and its gradient against FP64's
     hf = pkg.Handle(n, n)
@@ -483,23 +497,13 @@ def form_adjoint(args):
         hf.set_state(U)
         hf.advance(steps)
         f32_fwd.append(hf.run_stats()[0])
-    best32, grad32 = None, None
-    for _ in range(3):
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        hf.set_state(U)
-        torch.cuda.synchronize()
-        e0.record()
-        hf.forward(steps, ck)
-        e1.record()
-        grad32 = hf.vjp(cot)[..., 0]
-        e2.record()
-        torch.cuda.synchronize()
-        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
-        if best32 is None or sum(t) < sum(best32):
-            best32 = t
+    best32, grad32 = timed(hf, ck)
+    tape32 = timed(hf, pkg.FULL_TAPE)[0]
     hf.close()
     fp32 = {"forward_ms": min(f32_fwd), "forward_with_checkpoints_ms": best32[0], "vjp_ms": best32[1],
             "forward_plus_adjoint_over_forward": sum(best32) / min(f32_fwd),
+            "full_tape": {"forward_ms": tape32[0], "vjp_ms": tape32[1],
+                          "forward_plus_adjoint_over_forward": sum(tape32) / min(f32_fwd)},
             "gradient_rel_l2_vs_fp64": float(np.linalg.norm(grad32 - grad) / np.linalg.norm(grad)),
             "cotangent": "the FP64 run's"}
 
@@ -517,6 +521,7 @@ def form_adjoint(args):
     return {"form": "adjoint", "workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, 15 checkpoints",
             "forward_ms": fwd_ms, "forward_with_checkpoints_ms": ck_ms, "vjp_ms": vjp_ms,
             "forward_plus_adjoint_over_forward": (ck_ms + vjp_ms) / fwd_ms,
+            "full_tape": full_tape,
             "fd_check": {"direction": "6 smooth density modes", "eps": eps, "fd": fd, "adjoint": ad,
                          "rel_diff": abs(fd - ad) / abs(ad)},
             "fp32": fp32,

@@ -243,14 +243,24 @@ int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt);
 int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tangent_out, int stride);
 
 /* Advances the state nsteps steps keeping `checkpoints` evenly spaced
- * copies of it (sqrt(nsteps) is the usual choice) for fvm2d_vjp. */
+ * copies of it (sqrt(nsteps) is the usual choice) for fvm2d_vjp.
+ * checkpoints = FVM2D_FULL_TAPE keeps instead the whole tape: every step's
+ * input state, X(U), Y(U) and interface fluxes, 7 states per step (8.4 MB x 7
+ * per step at 512^2 in FP64), written by the forward steps themselves, so
+ * that fvm2d_vjp recomputes nothing and may be called several times for one
+ * forward.  Fails with FVM2D_ERR_INVALID when the tape does not fit in the
+ * device's free memory. */
+#define FVM2D_FULL_TAPE 0
 int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints);
 
 /* Adjoint of the last fvm2d_forward: given the cotangent of its final state,
  * returns in cotangent_out the cotangent of its initial state (the
- * vector-Jacobian product), recomputing each segment from its checkpoint and
- * running the hand-written reverse step backwards through it.  The state and
- * time are those after fvm2d_forward when it returns. */
+ * vector-Jacobian product), recomputing each segment from its checkpoint (or
+ * reading the full tape) and running the hand-written reverse step backwards
+ * through it.  The state and time are those after fvm2d_forward when it
+ * returns.  Changing a parameter (end time, CFL, alpha, gamma, preset,
+ * layout, precision, row frame, step size) after a full-tape forward
+ * discards its tape. */
 int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out, int stride);
 
 /* ---- batched form (no reference counterpart) -------------------------------

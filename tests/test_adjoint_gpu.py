@@ -18,6 +18,9 @@ can cross a switch.
 * The gradient of J = sum (rho_T - rho_target)^2 with respect to the initial
   density (the differentiation workload's objective, on a smaller array)
   matches central finite differences.
+* A full-tape forward (every step taped, nothing recomputed in the VJP) gives
+  the checkpointed run's state and cotangent, serves several VJPs, and is
+  discarded when a parameter changes.
 """
 import numpy as np
 import pytest
@@ -117,7 +120,7 @@ def test_dot_product_one_step_every_preset(pkg, oracle, strategy):
     assert abs(a - b) <= 1e-11 * max(abs(a), abs(b)), (a, b)
 
 
-@pytest.mark.parametrize("steps,checkpoints", [(12, 4), (25, 5), (7, 1)])
+@pytest.mark.parametrize("steps,checkpoints", [(12, 4), (25, 5), (7, 1), (25, 0)])
 def test_dot_product_many_steps_with_checkpoints(pkg, steps, checkpoints):
     U, w, h, hh = vortex_case(pkg, 96)
     dt = fixed_dt(pkg, U, hh)
@@ -238,3 +241,60 @@ def test_fp32_vjp_of_one_step_every_preset_agrees_with_fp64(pkg, oracle):
         rel = np.linalg.norm(out[1] - out[0]) / np.linalg.norm(out[0])
         print("preset", strategy, "fp32 vjp rel L2 vs fp64", rel)
         assert rel <= 1e-3, (strategy, rel)
+
+
+def diff_handle(pkg, U, w, h, dt, precision):
+    ny, nx = U.shape[:2]
+    hd = pkg.Handle(nx, ny)
+    hd.configure(w, h, 1e9, 0.45, 1.9, 1.4, 5, precision)
+    hd.set_fixed_dt(dt)
+    hd.set_state(U)
+    return hd
+
+
+# The ghost ring's transpose accumulates with atomics, so two VJPs of the
+# same tape may differ in the last bits: relative L2 bounds, not equality.
+@pytest.mark.parametrize("precision,tol", [("FP64", 1e-12), ("FP32", 1e-5)])
+def test_full_tape_matches_checkpoints(pkg, precision, tol):
+    n, steps = 96, 25
+    U, w, h, hh = vortex_case(pkg, n)
+    dt = fixed_dt(pkg, U, hh)
+    wv = np.random.default_rng(5).standard_normal(U.shape)
+    prec = getattr(pkg, precision)
+    out = {}
+    for ck in (5, pkg.FULL_TAPE):
+        hd = diff_handle(pkg, U, w, h, dt, prec)
+        hd.forward(steps, ck)
+        final = hd.get_state(4)
+        g = hd.vjp(wv)
+        assert np.array_equal(hd.get_state(4), final)  # the reverse leaves the final state in place
+        out[ck] = (final, g, hd.time_stages_count())
+        if ck == pkg.FULL_TAPE:
+            g2 = hd.vjp(2.0 * wv)  # the tape serves another cotangent without a new forward
+            rel = np.linalg.norm(g2 - 2.0 * g) / np.linalg.norm(2.0 * g)
+            assert rel <= tol, rel
+        hd.close()
+    (f5, g5, n5), (ft, gt, nt) = out[5], out[pkg.FULL_TAPE]
+    assert n5 == nt == steps
+    print(precision, "final state bit-identical:", np.array_equal(f5, ft))
+    assert np.allclose(ft, f5, rtol=tol, atol=0)
+    rel = np.linalg.norm(gt - g5) / np.linalg.norm(g5)
+    print(precision, "full tape vs checkpoints: cotangent rel L2", rel)
+    assert rel <= tol, rel
+
+
+def test_full_tape_is_discarded_by_a_parameter_change(pkg):
+    U, w, h, hh = vortex_case(pkg, 64)
+    dt = fixed_dt(pkg, U, hh)
+    hd = diff_handle(pkg, U, w, h, dt, pkg.FP64)
+    hd.forward(6, pkg.FULL_TAPE)
+    wv = np.ones_like(U)
+    hd.vjp(wv)
+    hd.configure(w, h, 1e9, 0.45, 1.8, 1.4, 5, pkg.FP64)  # alpha changed: the tape is stale
+    with pytest.raises(pkg.FVM2DError, match="call it first"):
+        hd.vjp(wv)
+    with pytest.raises(pkg.FVM2DError, match="use checkpoints"):
+        hd.forward(10**8, pkg.FULL_TAPE)  # rejected before any allocation
+    hd.forward(6, pkg.FULL_TAPE)
+    assert np.isfinite(hd.vjp(wv)).all()
+    hd.close()
