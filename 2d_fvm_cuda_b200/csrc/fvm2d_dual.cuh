@@ -49,6 +49,11 @@ __device__ __forceinline__ Dual sqrt(Dual a)
     const double r = ::sqrt(a.v);
     return Dual(r, a.d / (2.0 * r));
 }
+__device__ __forceinline__ Dual rrsqrt(Dual a)
+{
+    const double r = ::rsqrt(a.v);
+    return Dual(r, -0.5 * r * r * r * a.d);
+}
 __device__ __forceinline__ Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
 __device__ __forceinline__ Dual fma(Dual a, Dual b, Dual c) { return a * b + c; }
 

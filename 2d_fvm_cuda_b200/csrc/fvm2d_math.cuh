@@ -36,6 +36,10 @@ __device__ __forceinline__ Real rmax(Real a, Real b) { return (a < b) ? b : a; }
 // argument is NaN)
 __device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+// 1/sqrt(x): CUDA's rsqrt (1 ulp) and rsqrtf (2 ulp); the dual-number
+// overload lives with the dual type
+__device__ __forceinline__ double rrsqrt(double x) { return ::rsqrt(x); }
+__device__ __forceinline__ float rrsqrt(float x) { return ::rsqrtf(x); }
 
 // Generalized-minmod slope of one component from its left (m), centre (c)
 // and right (p) values.  src/basicFuns.cuh:49-68.
@@ -205,10 +209,13 @@ __device__ __forceinline__ Cell<Real> conservative_update(const Cell<Real> &U, c
 //
 // RefOrder: the reference's expressions in the reference's order (above).
 // Hoisted:  the same mathematics with the reciprocals hoisted and shared
-//           (1/rho_l, 1/rho_r, 1/(rho a) per side, 1/c_l, 1/c_r,
-//           1/(c_l + c_r), 1/rho_star: 8 divisions and 2 square roots per
-//           interface instead of 56 and 6), sqrt(g/(p rho)) rewritten as
-//           g/(rho a), and the midpoint flux written through the mass flux
+//           (1/rho_l and 1/rho_r from one division; 1/(rho a) per side as
+//           1/sqrt(g p rho), with a = g p/(rho a); the second side's 1/c and
+//           1/(c_l + c_r) from one division; 1/c of the first side and
+//           1/rho_star: 4 divisions and 2 reciprocal square roots per
+//           interface instead of 56 divisions and 6 square roots),
+//           sqrt(g/(p rho)) rewritten as g/(rho a), and the midpoint flux
+//           written through the mass flux
 //           m = rho u and its time derivative; the limiter tests signs on
 //           the raw differences and scales its minimum once, and h/2 is
 //           folded into the face states.  Rounding differs from the
@@ -322,26 +329,36 @@ struct Hoisted {
         const Real rho_lx = sL.rho, pi_lx = sL.p, u_lx = sL.un, v_lx = sL.ut;
         const Real rho_rx = sR.rho, pi_rx = sR.p, u_rx = sR.un, v_rx = sR.ut;
 
-        const Real irl = one / rho_l, irr = one / rho_r;
+        // 1/rho_l and 1/rho_r from one division
+        const Real irlr = one / (rho_l * rho_r);
+        const Real irl = rho_r * irlr, irr = rho_l * irlr;
         const Real e_l = pi_l * irl * igm1, e_r = pi_r * irr * igm1;
         const Real e_lx = (pi_lx - pi_l * rho_lx * irl) * irl * igm1;
         const Real e_rx = (pi_rx - pi_r * rho_rx * irr) * irr * igm1;
-        const Real a_l = sqrt(g * pi_l * irl), a_r = sqrt(g * pi_r * irr);
-        const Real il = one / (rho_l * a_l), ir = one / (rho_r * a_r);  // sqrt(g/(p rho)) = g/(rho a)
+        // 1/(rho a) = 1/sqrt(g p rho) and a = sqrt(g p / rho) = g p / sqrt(g p rho):
+        // one reciprocal square root per side
+        const Real il = rrsqrt(g * pi_l * rho_l), ir = rrsqrt(g * pi_r * rho_r);
+        const Real a_l = g * pi_l * il, a_r = g * pi_r * ir;
         const Real c_lx = half * g * (pi_l * rho_lx + rho_l * pi_lx) * il;
         const Real c_rx = half * g * (pi_r * rho_rx + rho_r * pi_rx) * ir;
         const Real du = u_l - u_r;
-        Real c_l, c_r, icl, icr;
+        // the side computed second gets its reciprocal and 1/(c_l + c_r)
+        // from one division
+        Real c_l, c_r, icl, icr, isum;
         if (pi_r >= pi_l) {
             c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) * ir + du));
             icl = one / c_l;
             c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) * icl + du));
-            icr = one / c_r;
+            const Real sc = c_l + c_r, q = one / (c_r * sc);
+            icr = sc * q;
+            isum = c_r * q;
         } else {
             c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) * il + du));
             icr = one / c_r;
             c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) * icr + du));
-            icl = one / c_l;
+            const Real sc = c_l + c_r, q = one / (c_l * sc);
+            icl = sc * q;
+            isum = c_l * q;
         }
         const Real sl = c_l * irl, sr = c_r * irr;  // c/rho: the fan's edge speeds relative to u
         Interface<Real> o;
@@ -360,7 +377,6 @@ struct Hoisted {
             o.ut_t = -u_r * v_rx;
             o.p_t = -u_r * pi_rx - c_r * sr * u_rx;
         } else {
-            const Real isum = one / (c_l + c_r);
             const Real u = (u_l * c_l + u_r * c_r + pi_l - pi_r) * isum;
             const Real pm = (du * c_l * c_r + c_l * pi_r + c_r * pi_l) * isum;
             const Real k_l = -pi_lx - c_l * u_lx - half * u_l * c_lx;

@@ -288,6 +288,7 @@ def product_arm(args, rank, world, local_rank):
             ref_cuda = {"value": n * n * rs / (loop_ms / 1e3), "unit": UNIT, "steps": rs,
                         "ms_per_step": loop_ms / rs, "timer": "its own loop timer (wrappers.cuh:193,286-288)",
                         "speedup_of_value": value / world / (n * n * rs / (loop_ms / 1e3))}
+        adjoint = adjoint_summary(pkg)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
@@ -313,6 +314,7 @@ def product_arm(args, rank, world, local_rank):
                              "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} four-quadrant, {csteps} steps in {cs:.1f} s"},
             "reference_cuda": ref_cuda,
             "fp32": fp32,
+            "adjoint": adjoint,
             "clocks": clocks,
             "gpu_launches": launches,
             "e2e_gpu_launches": e2e_launches,
@@ -416,6 +418,49 @@ def form_batch(args):
                            "1024 problems, sides 32..128")
     return {"form": "batch", "workload": "four-quadrant problems, t_end 0.2, each with its own dt",
             "results": results}
+
+
+def adjoint_summary(pkg):
+    """Forward + adjoint against forward on the differentiation workload
+    (512^2 periodic vortex + 16 density modes, 200 fixed-dt steps) with the
+    full tape, device-timed with CUDA events, best of three; the
+    finite-difference check and the checkpointed variant are in
+    --form adjoint."""
+    import torch
+    sc = pkg.scenarios
+    n, steps = 512, 200
+    w, hgt, hh = sc.periodic_square_layout(n)
+    U = sc.isentropic_vortex(n, perturbation=sc.density_modes(16, 1e-3, 3))
+    speed = np.sqrt(U[..., 2] ** 2 + U[..., 3] ** 2) + np.sqrt(1.4 * U[..., 1] / U[..., 0])
+    h = pkg.Handle(n, n)
+    h.configure(w, hgt, 1e9, 0.45, 1.9, 1.4, 5, pkg.FP64)
+    h.set_fixed_dt(0.45 * hh / speed.max())
+    fwd = []
+    for _ in range(4):
+        h.set_state(U)
+        h.advance(steps)
+        fwd.append(h.run_stats()[0])
+    cot = np.zeros_like(U)
+    cot[..., 0] = np.cos(np.arange(n))[None, :]
+    best = None
+    for _ in range(3):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        h.set_state(U)
+        torch.cuda.synchronize()
+        e0.record()
+        h.forward(steps, pkg.FULL_TAPE)
+        e1.record()
+        h.vjp(cot)
+        e2.record()
+        torch.cuda.synchronize()
+        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
+        if best is None or sum(t) < sum(best):
+            best = t
+    h.close()
+    f = min(fwd[1:])
+    return {"workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, FP64, full tape (11.7 GB)",
+            "forward_ms": f, "taped_forward_ms": best[0], "vjp_ms": best[1],
+            "forward_plus_adjoint_over_forward": sum(best) / f}
 
 
 def form_adjoint(args):
