@@ -288,7 +288,10 @@ def product_arm(args, rank, world, local_rank):
             ref_cuda = {"value": n * n * rs / (loop_ms / 1e3), "unit": UNIT, "steps": rs,
                         "ms_per_step": loop_ms / rs, "timer": "its own loop timer (wrappers.cuh:193,286-288)",
                         "speedup_of_value": value / world / (n * n * rs / (loop_ms / 1e3))}
-        adjoint = adjoint_summary(pkg)
+        try:  # a supplementary figure: a failure here must not lose the line
+            adjoint = adjoint_summary(pkg)
+        except Exception as e:  # noqa: BLE001
+            adjoint = {"error": f"{type(e).__name__}: {e}"}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
