@@ -1,0 +1,195 @@
+"""The sweep kernels' arithmetic policies checked against one another on the
+host (no GPU): tests/math_host.cpp compiles 2d_fvm_cuda_b200/csrc/
+fvm2d_math.cuh with g++ (contraction off) and exposes the relaxation GRP,
+the interface flux, the conservative update and the limited slopes of each
+policy.
+
+* Hoisted (the FP64 product build's shared reciprocals: 4 divisions and 2
+  reciprocal square roots per interface) equals RefOrder (the reference's
+  expressions and order, src/basicFuns.cuh:37-246) to rounding, in every wave
+  case of the GRP: the whole fan to the right, to the left, and the star
+  region on either side of the contact.
+* The same policy in single precision stays within FP32 rounding of the
+  double-precision reference order, and the compensated update
+  (HoistedCompensated, the FP32 build's) is more accurate than the plain one.
+* The slope limiter on raw differences picks exactly the reference's zero
+  pattern.
+
+Tolerances are normwise per component (errors divided by |value| plus the
+component's median magnitude), with the values measured on x86-64 in the
+comments.
+"""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CUDA_INC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+H, DT, GAMMA, ALPHA = 1 / 400, 0.4 / 400 / 8, 1.4, 1.9
+K4 = (H, DT, GAMMA, ALPHA)
+
+
+@pytest.fixture(scope="module")
+def mh(tmp_path_factory):
+    if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INC, "cuda_runtime.h")):
+        pytest.skip("needs g++ and the CUDA headers")
+    so = str(tmp_path_factory.mktemp("math_host") / "libmath_host.so")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I", CUDA_INC,
+                    os.path.join(HERE, "math_host.cpp"), "-o", so], check=True)
+    lib = ctypes.CDLL(so)
+    for f in ("mh_grp", "mh_flux", "mh_update", "mh_slope"):
+        getattr(lib, f).argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p]
+        getattr(lib, f).restype = ctypes.c_int
+
+    def call(name, policy, bits, X, k4=K4):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        k = np.asarray(k4, dtype=np.float64)
+        width = {"mh_grp": 10}.get(name, 4)
+        out = np.empty((X.shape[0], width))
+        assert getattr(lib, name)(policy, bits, X.shape[0], X.ctypes.data, k.ctypes.data, out.ctypes.data) == 0
+        return out
+
+    return call
+
+
+REF, HOISTED, COMPENSATED = 0, 1, 2
+
+
+def cells(rng, n):
+    """rho in [0.1, 3] and p in [0.05, 5] (log-uniform), u in [-4, 4],
+    v in [-2, 2]: sub- and supersonic states with pressure ratios up to 100."""
+    rho = np.exp(rng.uniform(np.log(0.1), np.log(3.0), n))
+    p = np.exp(rng.uniform(np.log(0.05), np.log(5.0), n))
+    return np.stack([rho, p, rng.uniform(-4, 4, n), rng.uniform(-2, 2, n)], 1)
+
+
+def interfaces(seed, n=100_000):
+    rng = np.random.default_rng(seed)
+    L, R = cells(rng, n), cells(rng, n)
+    sL = rng.standard_normal((n, 4)) * L * 0.5
+    sR = rng.standard_normal((n, 4)) * R * 0.5
+    return L, R, np.concatenate([L, R, sL, sR], 1)
+
+
+def normwise(A, B):
+    """max over samples of |A - B| / (|B| + median |B|), per component."""
+    return (np.abs(A - B) / (np.abs(B) + np.median(np.abs(B), 0))).max(0)
+
+
+def test_hoisted_grp_equals_reference_order_in_every_wave_case(mh):
+    L, R, X = interfaces(1)
+    W0 = mh("mh_grp", REF, 64, X)
+    W1 = mh("mh_grp", HOISTED, 64, X)
+    left = (W0[:, 0] == L[:, 0]) & (W0[:, 2] == L[:, 2])
+    right = (W0[:, 0] == R[:, 0]) & (W0[:, 2] == R[:, 2])
+    star = ~left & ~right
+    n = len(X)
+    for name, sel in (("fan right", left), ("fan left", right), ("star, u <= 0", star & (W0[:, 2] <= 0)),
+                      ("star, u > 0", star & (W0[:, 2] > 0)), ("p_R >= p_L", R[:, 1] >= L[:, 1]),
+                      ("p_R < p_L", R[:, 1] < L[:, 1])):
+        assert sel.sum() > n // 20, name  # every branch well covered
+        e = normwise(W1[sel], W0[sel])
+        print(name, sel.sum(), "max normwise", e.max())
+        assert e.max() <= 1e-13, (name, e)  # measured 1.9e-14 (the time derivatives)
+
+
+def test_hoisted_flux_equals_reference_order(mh):
+    _, _, X = interfaces(2)
+    F0 = mh("mh_flux", REF, 64, X)
+    F1 = mh("mh_flux", HOISTED, 64, X)
+    e = normwise(F1, F0)
+    print("flux FP64 normwise", e)
+    assert e.max() <= 1e-13, e  # measured 7.2e-15
+
+
+def test_uniform_state_is_a_fixed_point(mh):
+    """Equal face states and zero slopes: the interface state is the cell's
+    and every time derivative is zero, in both policies and precisions."""
+    rng = np.random.default_rng(3)
+    C = cells(rng, 20_000)
+    X = np.concatenate([C, C, np.zeros_like(C), np.zeros_like(C)], 1)
+    for policy in (REF, HOISTED):
+        for bits in (64, 32):
+            W = mh("mh_grp", policy, bits, X)
+            Cb = C if bits == 64 else C.astype(np.float32).astype(np.float64)
+            # the star region recombines u and p from both sides: a few
+            # roundings (measured 5.3e-16 in FP64, 2.7e-7 in FP32)
+            e = normwise(W[:, :4], Cb)
+            assert e.max() <= (4e-15 if bits == 64 else 1e-6), (policy, bits, e)
+            assert np.all(W[:, 5:] == 0.0), (policy, bits)
+
+
+def test_fp32_grp_and_flux_stay_within_single_precision_rounding(mh):
+    _, _, X = interfaces(4)
+    X32 = X.astype(np.float32).astype(np.float64)  # the FP32 build's inputs
+    e = normwise(mh("mh_grp", HOISTED, 32, X32), mh("mh_grp", REF, 64, X32))
+    print("grp FP32 vs FP64 normwise", e)
+    assert e.max() <= 1e-4, e  # measured 1.3e-5 (energy derivative)
+    e = normwise(mh("mh_flux", HOISTED, 32, X32), mh("mh_flux", REF, 64, X32))
+    print("flux FP32 vs FP64 normwise", e)
+    assert e.max() <= 5e-5, e  # measured 5.4e-6
+
+
+def update_inputs(seed, n=100_000):
+    rng = np.random.default_rng(seed)
+    U = cells(rng, n)
+    FL = rng.standard_normal((n, 4))
+    FR = FL + 0.5 * rng.standard_normal((n, 4))
+    # values an FP32 sweep holds: every input exactly representable in FP32
+    return np.concatenate([U, FL, FR], 1).astype(np.float32).astype(np.float64)
+
+
+def update_errors(P, R):
+    """Errors of primitives P against R scaled as the conserved variables
+    carry them: rho relative, p against (gamma - 1) E, velocities against
+    |u| + |v| + sqrt(p / rho)."""
+    rho, p, u, v = R.T
+    E = p / (GAMMA - 1) + 0.5 * rho * (u * u + v * v)
+    vel = np.abs(u) + np.abs(v) + np.sqrt(np.abs(p) / rho)
+    return np.stack([np.abs(P[:, 0] - rho) / rho, np.abs(P[:, 1] - p) / ((GAMMA - 1) * E),
+                     np.abs(P[:, 2] - u) / vel, np.abs(P[:, 3] - v) / vel], 1)
+
+
+def test_updates_agree_and_compensation_helps_in_fp32(mh):
+    X = update_inputs(5)
+    k32 = (float(np.float32(H)), float(np.float32(DT)), GAMMA, ALPHA)  # lambda as the FP32 build forms it
+    R0 = mh("mh_update", REF, 64, X, k32)
+    ok = (R0[:, 0] > 0) & (R0[:, 1] > 0)
+    assert ok.mean() > 0.8
+    for policy in (HOISTED, COMPENSATED):
+        e = update_errors(mh("mh_update", policy, 64, X, k32), R0)[ok].max(0)
+        print("FP64 update policy", policy, e)
+        assert e.max() <= 4e-15, (policy, e)  # measured 5.5e-16
+    plain = update_errors(mh("mh_update", HOISTED, 32, X, k32), R0)[ok]
+    comp = update_errors(mh("mh_update", COMPENSATED, 32, X, k32), R0)[ok]
+    print("FP32 plain update: max", plain.max(0), "mean", plain.mean(0))
+    print("FP32 compensated update: max", comp.max(0), "mean", comp.mean(0))
+    # compensated: about the final rounding to FP32 (measured max 2.9e-7 for
+    # rho, 1.1-1.6e-7 for p, u, v; plain: up to 4.1e-7)
+    assert comp.max(0)[0] <= 4e-7 and comp.max(0)[1:].max() <= 3e-7, comp.max(0)
+    # and smaller on average than the plain FP32 update for p, u and v
+    # (measured 0.59, 0.64, 0.63 of it)
+    assert np.all(comp.mean(0)[1:] <= 0.8 * plain.mean(0)[1:]), (comp.mean(0), plain.mean(0))
+
+
+def test_hoisted_limiter_picks_the_reference_zero_pattern(mh):
+    rng = np.random.default_rng(6)
+    n = 100_000
+    X = np.concatenate([cells(rng, n), cells(rng, n), cells(rng, n)], 1)
+    S0 = mh("mh_slope", REF, 64, X)
+    S1 = mh("mh_slope", HOISTED, 64, X)
+    nz = S0 != 0
+    assert 0.2 < nz.mean() < 0.5
+    assert np.array_equal(nz, S1 != 0)
+    assert (np.abs(S1 - S0)[nz] / np.abs(S0[nz])).max() <= 1e-15  # measured 2.3e-16
+    X32 = X.astype(np.float32).astype(np.float64)
+    S0 = mh("mh_slope", REF, 64, X32)
+    S1 = mh("mh_slope", HOISTED, 32, X32)
+    nz = S0 != 0
+    assert np.array_equal(nz, S1 != 0)
+    assert (np.abs(S1 - S0)[nz] / np.abs(S0[nz])).max() <= 4e-7  # measured 1.1e-7
