@@ -6,17 +6,30 @@
 // and in single precision.  tests/test_math_host.py builds it and calls it
 // through ctypes.
 //
+// It also holds the hand-written adjoint of the interface flux, the update
+// and the limiter (csrc/fvm2d_adjoint_math.cuh) and a dual-number tangent of
+// the forward (csrc/fvm2d_dual.cuh), for a per-interface dot-product test of
+// the adjoint.
+//
 // The device code takes 1/sqrt(x) from CUDA's rsqrt/rsqrtf, which exist only
-// in device code; here they are 1/sqrt(x) in the host's arithmetic.
+// in device code; here they are 1/sqrt(x) in the host's arithmetic.  The
+// dual type's warp shuffles are declared for the compiler and never called.
 #include <cmath>
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+template <typename T>
+static inline T __shfl_down_sync(unsigned, T v, int) { return v; }
+template <typename T>
+static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 
 #define FVM2D_VARIANT host
-#include "../2d_fvm_cuda_b200/csrc/fvm2d_math.cuh"
+#define FVM2D_REAL double
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint_math.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
 
 using namespace fvm2d::host;
+using fvm2d::ad::Dual;
 
 namespace {
 
@@ -130,6 +143,19 @@ int slope_n(int policy, long n, const double *in, const double *k4, double *out)
     return 0;
 }
 
+Cell<Dual> dual_cell(const double *p, const double *d)
+{
+    return Cell<Dual>{Dual(p[0], d[0]), Dual(p[1], d[1]), Dual(p[2], d[2]), Dual(p[3], d[3])};
+}
+
+void put_tangent(const Cell<Dual> &c, double *o)
+{
+    o[0] = c.rho.d;
+    o[1] = c.p.d;
+    o[2] = c.un.d;
+    o[3] = c.ut.d;
+}
+
 } // namespace
 
 // Every entry: `policy` 0 = RefOrder, 1 = Hoisted, 2 = HoistedCompensated
@@ -169,6 +195,99 @@ int mh_slope(int policy, int bits, long n, const double *in, const double *k4, d
     if (bits == 64) return slope_n<double>(policy, n, in, k4, out);
     if (bits == 32) return slope_n<float>(policy, n, in, k4, out);
     return 1;
+}
+
+// ---- derivatives (FP64, shared-reciprocal forms) ----------------------------
+// Tangents (dual numbers through Hoisted) and adjoints (the hand-written
+// reverse the VJP kernels run) of the same maps, one interface or cell per
+// row.  dir / w are the tangent directions / output adjoints, in the layout
+// of the inputs / outputs above.
+
+// d flux: in, dir n x 16 -> out n x 4
+int mh_flux_jvp(long n, const double *in, const double *dir, const double *k4, double *out)
+{
+    const SweepConsts<Dual> K = consts<Dual>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 16 * i, *d = dir + 16 * i;
+        put_tangent(Hoisted::interface_flux(dual_cell(p, d), dual_cell(p + 4, d + 4), dual_cell(p + 8, d + 8),
+                                            dual_cell(p + 12, d + 12), K),
+                    out + 4 * i);
+    }
+    return 0;
+}
+
+// flux adjoint: in n x 16, w n x 4 -> out n x 16
+int mh_flux_vjp(long n, const double *in, const double *w, const double *k4, double *out)
+{
+    const SweepConsts<double> K = consts<double>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 16 * i;
+        Cell<double> b[4] = {};
+        interface_flux_adjoint(cell<double>(p), cell<double>(p + 4), cell<double>(p + 8), cell<double>(p + 12), K,
+                               cell<double>(w + 4 * i), b[0], b[1], b[2], b[3]);
+        for (int q = 0; q < 4; ++q) put(b[q], out + 16 * i + 4 * q);
+    }
+    return 0;
+}
+
+// d update: in, dir n x 12 (U, F_L, F_R) -> out n x 4
+int mh_update_jvp(long n, const double *in, const double *dir, const double *k4, double *out)
+{
+    const SweepConsts<Dual> K = consts<Dual>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 12 * i, *d = dir + 12 * i;
+        put_tangent(Hoisted::update(dual_cell(p, d), dual_cell(p + 4, d + 4), dual_cell(p + 8, d + 8), K),
+                    out + 4 * i);
+    }
+    return 0;
+}
+
+// update adjoint: in n x 12, w n x 4 -> out n x 12 (U, F_L, F_R); the flux
+// adjoints are +lambda and -lambda times the conserved vector's adjoint
+int mh_update_vjp(long n, const double *in, const double *w, const double *k4, double *out)
+{
+    const SweepConsts<double> K = consts<double>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 12 * i;
+        double *o = out + 12 * i;
+        Cell<double> Ub = {};
+        const Cell<double> mb = update_adjoint(cell<double>(p), cell<double>(p + 4), cell<double>(p + 8), K,
+                                               cell<double>(w + 4 * i), Ub);
+        put(Ub, o);
+        const Cell<double> fl = {K.lambda * mb.rho, K.lambda * mb.p, K.lambda * mb.un, K.lambda * mb.ut};
+        put(fl, o + 4);
+        const Cell<double> fr = {-fl.rho, -fl.p, -fl.un, -fl.ut};
+        put(fr, o + 8);
+    }
+    return 0;
+}
+
+// d slopes: in, dir n x 12 (left, centre, right) -> out n x 4
+int mh_slope_jvp(long n, const double *in, const double *dir, const double *k4, double *out)
+{
+    const SweepConsts<Dual> K = consts<Dual>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 12 * i, *d = dir + 12 * i;
+        put_tangent(Hoisted::slope(dual_cell(p, d), dual_cell(p + 4, d + 4), dual_cell(p + 8, d + 8), K),
+                    out + 4 * i);
+    }
+    return 0;
+}
+
+// slope adjoint: in n x 12, w n x 4 -> out n x 12
+int mh_slope_vjp(long n, const double *in, const double *w, const double *k4, double *out)
+{
+    const SweepConsts<double> K = consts<double>(k4);
+    for (long i = 0; i < n; ++i) {
+        const double *p = in + 12 * i, *wi = w + 4 * i;
+        double *o = out + 12 * i;
+        for (int q = 0; q < 12; ++q) o[q] = 0.0;
+        for (int f = 0; f < 4; ++f) {
+            const int ch = slope_choice(p[f], p[4 + f], p[8 + f], K.rh, K.alpha);
+            slope_adjoint(ch, wi[f], K.rh, K.alpha, o[f], o[4 + f], o[8 + f]);
+        }
+    }
+    return 0;
 }
 
 } // extern "C"
