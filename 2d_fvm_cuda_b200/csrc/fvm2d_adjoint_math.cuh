@@ -102,39 +102,47 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
     const A u_r = fma(-sR.un, hh, UR.un), v_r = fma(-sR.ut, hh, UR.ut);
     const A rho_lx = sL.rho, pi_lx = sL.p, u_lx = sL.un, v_lx = sL.ut;
     const A rho_rx = sR.rho, pi_rx = sR.p, u_rx = sR.un, v_rx = sR.ut;
-    // ---- forward: Hoisted::grp ----
-    const A irl = one / rho_l, irr = one / rho_r;
+    // ---- forward: Hoisted::grp, its reciprocals formed as it forms them
+    // (the reverse below uses only what they are: irl = 1/rho_l,
+    // il = 1/(rho_l a_l), a_l = sqrt(g pi_l / rho_l), icl = 1/c_l,
+    // isum = 1/(c_l + c_r), and the same on the right) ----
+    const A irlr = one / (rho_l * rho_r);
+    const A irl = rho_r * irlr, irr = rho_l * irlr;
     const A e_l = pi_l * irl * igm1, e_r = pi_r * irr * igm1;
     const A X_l = pi_lx - pi_l * rho_lx * irl, X_r = pi_rx - pi_r * rho_rx * irr;
     const A e_lx = X_l * irl * igm1, e_rx = X_r * irr * igm1;
-    const A a_l = sqrt(g * pi_l * irl), a_r = sqrt(g * pi_r * irr);
-    const A il = one / (rho_l * a_l), ir = one / (rho_r * a_r);
+    const A il = rrsqrt(g * pi_l * rho_l), ir = rrsqrt(g * pi_r * rho_r);
+    const A a_l = g * pi_l * il, a_r = g * pi_r * ir;
     const A Y_l = pi_l * rho_lx + rho_l * pi_lx, Y_r = pi_r * rho_rx + rho_r * pi_rx;
     const A c_lx = half * g * Y_l * il, c_rx = half * g * Y_r * ir;
     const A du = u_l - u_r;
     const bool right_first = pi_r >= pi_l;
-    A zl_arg, zr_arg, c_l, c_r, icl, icr;
+    A zl_arg, zr_arg, c_l, c_r, icl, icr, isum;
     if (right_first) {
         zl_arg = (pi_r - pi_l) * ir + du;
         c_l = rho_l * (a_l + kappa * rmax(zero, zl_arg));
         icl = one / c_l;
         zr_arg = (pi_l - pi_r) * icl + du;
         c_r = rho_r * (a_r + kappa * rmax(zero, zr_arg));
-        icr = one / c_r;
+        const A sc = c_l + c_r, q = one / (c_r * sc);
+        icr = sc * q;
+        isum = c_r * q;
     } else {
         zr_arg = (pi_l - pi_r) * il + du;
         c_r = rho_r * (a_r + kappa * rmax(zero, zr_arg));
         icr = one / c_r;
         zl_arg = (pi_r - pi_l) * icr + du;
         c_l = rho_l * (a_l + kappa * rmax(zero, zl_arg));
-        icl = one / c_l;
+        const A sc = c_l + c_r, q = one / (c_l * sc);
+        icl = sc * q;
+        isum = c_l * q;
     }
     const A zl = rmax(zero, zl_arg), zr = rmax(zero, zr_arg);
     const A sl = c_l * irl, sr = c_r * irr;
     const int wave = (u_l - sl >= zero) ? 0 : ((u_r + sr <= zero) ? 1 : 2);  // left, right, star
     Cell5 W, Wt;
     // star-region intermediates (used only when wave == 2)
-    A isum = 0, u = 0, pm = 0, k_l = 0, k_r = 0, H = 0, G = 0, d_l = 0, d_r = 0, Dp = 0;
+    A u = 0, pm = 0, k_l = 0, k_r = 0, H = 0, G = 0, d_l = 0, d_r = 0, Dp = 0;
     A irho = 0, rho = 0, ic2 = 0, rho3 = 0, urho = 0, A1 = 0, B1 = 0, C1 = 0, P = 0, V = 0, Q = 0, T1 = 0, T2 = 0;
     bool star_right = false;
     if (wave == 0) {
@@ -152,7 +160,6 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
         Wt.ut = -u_r * v_rx;
         Wt.p = -u_r * pi_rx - c_r * sr * u_rx;
     } else {
-        isum = one / (c_l + c_r);
         u = (u_l * c_l + u_r * c_r + pi_l - pi_r) * isum;
         pm = (du * c_l * c_r + c_l * pi_r + c_r * pi_l) * isum;
         k_l = -pi_lx - c_l * u_lx - half * u_l * c_lx;
