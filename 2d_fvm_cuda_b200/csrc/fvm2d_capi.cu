@@ -11,8 +11,9 @@
 //   is one 64-byte read per graph replay (the reference reads the max wave
 //   speed back and synchronizes 17 times per step, src/wrappers.cuh:196-284);
 //   and, allocated on first use, the differentiation workspaces (dual-number
-//   states of fvm2d_jvp; checkpoints, one segment's tape and the adjoint
-//   states of fvm2d_forward / fvm2d_vjp, with graphs of a full segment).
+//   states of fvm2d_jvp; checkpoints, one segment's tape (or, for a
+//   full-tape forward, every step's) and the adjoint states of
+//   fvm2d_forward / fvm2d_vjp, with graphs of a full segment).
 #include "../../include/fvm2d.h"
 #include "fvm2d_io.cuh"
 #include "fvm2d_adjoint.h"
