@@ -11,13 +11,24 @@
 // the forward (csrc/fvm2d_dual.cuh), for a per-interface dot-product test of
 // the adjoint.
 //
-// The device code takes 1/sqrt(x) from CUDA's rsqrt/rsqrtf, which exist only
-// in device code; here they are 1/sqrt(x) in the host's arithmetic.  The
-// dual type's warp shuffles are declared for the compiler and never called.
+// The device code takes 1/sqrt(x) from CUDA's rsqrt/rsqrtf and the FP32 build
+// its paired single-precision operations from sm_100's two-wide instructions,
+// which exist only in device code; here they are 1/sqrt(x) and two
+// correctly rounded scalar operations (what the two-wide instructions do
+// lane by lane).  The dual type's warp shuffles are declared for the
+// compiler and never called.
 #include <cmath>
+
+#include <cuda_runtime.h>
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+static inline float2 __fadd2_rn(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+static inline float2 __fmul2_rn(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+static inline float2 __ffma2_rn(float2 a, float2 b, float2 c)
+{
+    return make_float2(std::fma(a.x, b.x, c.x), std::fma(a.y, b.y, c.y));
+}
 template <typename T>
 static inline T __shfl_down_sync(unsigned, T v, int) { return v; }
 template <typename T>
@@ -27,6 +38,7 @@ static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 #define FVM2D_REAL double
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint_math.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
 
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
@@ -101,8 +113,12 @@ int flux_n(int policy, long n, const double *in, const double *k4, double *out)
             put(RefOrder::interface_flux(UL, UR, sL, sR, K), out + 4 * i);
         else if (policy == 1)
             put(Hoisted::interface_flux(UL, UR, sL, sR, K), out + 4 * i);
-        else
+        else if constexpr (sizeof(Real) == 4) {
+            if (policy != 3) return 1;
+            put(PackedCompensated::interface_flux(UL, UR, sL, sR, K), out + 4 * i);
+        } else {
             return 1;
+        }
     }
     return 0;
 }
@@ -120,8 +136,12 @@ int update_n(int policy, long n, const double *in, const double *k4, double *out
             put(Hoisted::update(U, FL, FR, K), out + 4 * i);
         else if (policy == 2)
             put(HoistedCompensated::update(U, FL, FR, K), out + 4 * i);
-        else
+        else if constexpr (sizeof(Real) == 4) {
+            if (policy != 3) return 1;
+            put(PackedCompensated::update(U, FL, FR, K), out + 4 * i);
+        } else {
             return 1;
+        }
     }
     return 0;
 }
@@ -159,7 +179,9 @@ void put_tangent(const Cell<Dual> &c, double *o)
 } // namespace
 
 // Every entry: `policy` 0 = RefOrder, 1 = Hoisted, 2 = HoistedCompensated
-// (update only); `bits` 64 or 32 is the arithmetic (inputs rounded to it);
+// (update only), 3 = PackedCompensated (flux and update, 32 bits only: the
+// FP32 build's physics); `bits` 64 or 32 is the arithmetic (inputs rounded
+// to it);
 // k4 = (h, dt, gamma, alpha).  Returns 0, or 1 for an unknown policy/bits.
 extern "C" {
 
