@@ -9,9 +9,11 @@ The package directory name starts with a digit, so import it with
   want the state to stay on the GPU between calls.
 * ``Batch`` -- many independent problems of different sizes solved together.
 * ``slab`` -- one problem split by rows across processes (one GPU each).
+* ``ensemble`` -- many independent problems dealt out whole across processes
+  (one GPU each), each rank's share solved as one batch.
 * ``scenarios`` -- initial data (the reference's demo problems and seeded
   workloads).
 """
-from . import scenarios, slab  # noqa: F401
+from . import ensemble, scenarios, slab  # noqa: F401
 from ._lib import FP32, FP64, FP64_REFORDER, FP64_STRICT, FULL_TAPE, Batch, FVM2DError, Handle, LIB_PATH, load  # noqa: F401
 from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

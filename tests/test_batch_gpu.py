@@ -102,3 +102,15 @@ def test_strict_batch_equals_oracle(pkg, oracle):
                                                               "strategy")})
         assert got[p][1:] == (steps, t)
         assert np.array_equal(got[p][0], O, equal_nan=True)
+
+
+def test_ensemble_without_a_process_group_is_one_batch(pkg, oracle):
+    """2d_fvm_cuda_b200.ensemble on a single process: its default share
+    solver runs the whole list as one batch, bit for bit the batch above."""
+    probs = problems(pkg, oracle)
+    want, _ = batch_solve(pkg, probs, 1)
+    E = pkg.ensemble.EnsembleSolver(probs, precision=1)
+    assert E.solve() == len(probs)
+    for (G, steps, t), (V, tt, ss) in zip(want, E.gather()):
+        assert (ss, tt) == (steps, t)
+        assert np.array_equal(V, G, equal_nan=True)
