@@ -1,7 +1,8 @@
 """Row-slab decomposition of one problem across processes (2d_fvm_cuda_b200/slab.py),
 tested on CPU: gloo ranks whose slabs are stepped by the oracle-backed
-stand-in of tests/slab_ranks.py.  The gathered result must equal the oracle's
-single-array run bit for bit: same steps, same time, same cells."""
+stand-in of tests/slab_ranks.py, on every ghost preset.  The gathered result
+must equal the oracle's single-array run bit for bit: same steps, same time,
+same cells."""
 import socket
 
 import numpy as np
@@ -53,6 +54,12 @@ CASES = [
     dict(world=2, nx=64, ny=57, seed=3, strategy=0, width=1.0, height=1.1, t_end=0.05, steps=12),
     dict(world=3, nx=33, ny=46, seed=4, strategy=5, width=1.0, height=1.0, t_end=0.05, steps=12),
     dict(world=2, nx=40, ny=30, seed=5, strategy=6, width=1.2, height=1.0, t_end=0.05, steps=12),
+    # presets whose ghost rules read global row numbers (double-Mach shock
+    # position, jet inflow rows)
+    dict(world=3, nx=48, ny=40, seed=6, strategy=4, width=1.0, height=1.0, t_end=0.02, steps=10),
+    dict(world=2, nx=48, ny=42, seed=7, strategy=1, width=1.0, height=1.0, t_end=0.02, steps=10),
+    dict(world=3, nx=40, ny=50, seed=8, strategy=2, width=1.0, height=1.0, t_end=0.001, steps=10),
+    dict(world=2, nx=40, ny=44, seed=9, strategy=3, width=1.0, height=1.0, t_end=0.001, steps=10),
 ]
 
 
