@@ -213,7 +213,9 @@ __device__ __forceinline__ Cell<Real> conservative_update(const Cell<Real> &U, c
 //           1/sqrt(g p rho), with a = g p/(rho a); the second side's 1/c and
 //           1/(c_l + c_r) from one division; 1/c of the first side and
 //           1/rho_star: 4 divisions and 2 reciprocal square roots per
-//           interface instead of 56 divisions and 6 square roots),
+//           interface in the star region, 3 and 2 when the wave fan is
+//           one-sided, where the reference's expressions divide by a
+//           variable 61 times (27-28) and take 4 square roots),
 //           sqrt(g/(p rho)) rewritten as g/(rho a), and the midpoint flux
 //           written through the mass flux
 //           m = rho u and its time derivative; the limiter tests signs on

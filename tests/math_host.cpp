@@ -40,6 +40,38 @@ static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
 
+// A number that counts the operations done on it, to state how many
+// divisions and square roots each policy spends per interface.
+namespace opcount {
+struct Counts {
+    long add, mul, div, div2, sqrt, rsqrt, fma, cmp;  // div2: divisions by the constant 2 (a compiler makes them products)
+};
+static Counts g_counts;
+struct Num {
+    double v;
+    Num() : v(0.0) {}
+    Num(double x) : v(x) {}
+    explicit operator double() const { return v; }
+};
+inline Num operator+(Num a, Num b) { ++g_counts.add; return Num(a.v + b.v); }
+inline Num operator-(Num a, Num b) { ++g_counts.add; return Num(a.v - b.v); }
+inline Num operator-(Num a) { return Num(-a.v); }
+inline Num operator*(Num a, Num b) { ++g_counts.mul; return Num(a.v * b.v); }
+inline Num operator/(Num a, Num b)
+{
+    ++(b.v == 2.0 ? g_counts.div2 : g_counts.div);
+    return Num(a.v / b.v);
+}
+inline bool operator<(Num a, Num b) { ++g_counts.cmp; return a.v < b.v; }
+inline bool operator>(Num a, Num b) { ++g_counts.cmp; return a.v > b.v; }
+inline bool operator<=(Num a, Num b) { ++g_counts.cmp; return a.v <= b.v; }
+inline bool operator>=(Num a, Num b) { ++g_counts.cmp; return a.v >= b.v; }
+inline Num sqrt(Num a) { ++g_counts.sqrt; return Num(std::sqrt(a.v)); }
+inline Num rrsqrt(Num a) { ++g_counts.rsqrt; return Num(1.0 / std::sqrt(a.v)); }
+inline Num fabs(Num a) { return Num(std::fabs(a.v)); }
+inline Num fma(Num a, Num b, Num c) { ++g_counts.fma; return Num(std::fma(a.v, b.v, c.v)); }
+} // namespace opcount
+
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
 
@@ -309,6 +341,35 @@ int mh_slope_vjp(long n, const double *in, const double *w, const double *k4, do
             slope_adjoint(ch, wi[f], K.rh, K.alpha, o[f], o[4 + f], o[8 + f]);
         }
     }
+    return 0;
+}
+
+// Operations of one evaluation for policy 0 = RefOrder or 1 = Hoisted:
+// what = 0 the GRP alone (face states in, 16 doubles as for mh_grp), 1 the
+// whole interface flux (cells and slopes in, as for mh_flux: face states,
+// GRP, midpoint flux).  counts: additions and subtractions,
+// multiplications, divisions (by a variable), divisions by the constant 2,
+// square roots, reciprocal square roots, fused multiply-adds, comparisons.  Constant operands formed once per sweep
+// (SweepConsts) are not counted.
+int mh_count(int policy, int what, const double *in, const double *k4, long *counts)
+{
+    using opcount::Num;
+    const Cell<Num> L = cell<Num>(in), R = cell<Num>(in + 4), sL = cell<Num>(in + 8), sR = cell<Num>(in + 12);
+    const SweepConsts<Num> K = consts<Num>(k4);
+    opcount::g_counts = {};
+    if (policy == 0 && what == 0)
+        relaxation_grp(L, R, sL, sR, K.g);
+    else if (policy == 1 && what == 0)
+        Hoisted::grp(L, R, sL, sR, K);
+    else if (policy == 0 && what == 1)
+        RefOrder::interface_flux(L, R, sL, sR, K);
+    else if (policy == 1 && what == 1)
+        Hoisted::interface_flux(L, R, sL, sR, K);
+    else
+        return 1;
+    const opcount::Counts &c = opcount::g_counts;
+    const long v[8] = {c.add, c.mul, c.div, c.div2, c.sqrt, c.rsqrt, c.fma, c.cmp};
+    for (int i = 0; i < 8; ++i) counts[i] = v[i];
     return 0;
 }
 

@@ -16,6 +16,10 @@ policy.
   gives the same results as the scalar form.
 * The slope limiter on raw differences picks exactly the reference's zero
   pattern.
+* The operations each policy spends per interface, counted per wave case
+  with a counting number type: the shared-reciprocal form's 4 divisions and
+  2 reciprocal square roots (3 and 2 when the fan is one-sided) against the
+  reference expressions' 61 divisions by a variable and 4 square roots.
 * The hand-written adjoint that the VJP kernels run (interface flux, update,
   limiter; csrc/fvm2d_adjoint_math.cuh) is the transpose of the forward's
   tangent: per interface, <J v, w> = <v, J^T w> with J v from dual numbers
@@ -51,6 +55,16 @@ def mh(tmp_path_factory):
         getattr(lib, f).argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]
         getattr(lib, f).restype = ctypes.c_int
+    lib.mh_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.mh_count.restype = ctypes.c_int
+
+    def count(policy, what, x, k4=K4):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        k = np.asarray(k4, dtype=np.float64)
+        c = np.zeros(8, dtype=np.int64)
+        assert lib.mh_count(policy, what, x.ctypes.data, k.ctypes.data, c.ctypes.data) == 0
+        return dict(zip(("add", "mul", "div", "div2", "sqrt", "rsqrt", "fma", "cmp"), c.tolist()))
+
     for f in ("mh_flux_jvp", "mh_flux_vjp", "mh_update_jvp", "mh_update_vjp", "mh_slope_jvp", "mh_slope_vjp"):
         getattr(lib, f).argtypes = [ctypes.c_long] + [ctypes.c_void_p] * 4
         getattr(lib, f).restype = ctypes.c_int
@@ -73,6 +87,7 @@ def mh(tmp_path_factory):
         return out
 
     call.deriv = deriv
+    call.count = count
     return call
 
 
@@ -115,6 +130,33 @@ def test_hoisted_grp_equals_reference_order_in_every_wave_case(mh):
         e = normwise(W1[sel], W0[sel])
         print(name, sel.sum(), "max normwise", e.max())
         assert e.max() <= 1e-13, (name, e)  # measured 1.9e-14 (the time derivatives)
+
+
+def wave_cases(W, L, R):
+    """0: the fan moves right (left state), 1: left (right state), 2: star
+    region with u <= 0, 3: star region with u > 0."""
+    left = (W[:, 0] == L[:, 0]) & (W[:, 2] == L[:, 2])
+    right = (W[:, 0] == R[:, 0]) & (W[:, 2] == R[:, 2])
+    return np.where(left, 0, np.where(right, 1, np.where(W[:, 2] <= 0, 2, 3)))
+
+
+def test_divisions_and_square_roots_per_interface(mh):
+    """Counted per wave case on 2000 interfaces, for the whole interface flux
+    (face states, GRP, midpoint flux); counts are the same for every
+    interface of a case."""
+    L, R, X = interfaces(1, 2000)
+    case = wave_cases(mh("mh_grp", REF, 64, X), L, R)
+    want = {  # (policy, case): (divisions by a variable, halvings, sqrt, rsqrt)
+        (REF, 0): (27, 10, 4, 0), (REF, 1): (28, 10, 4, 0), (REF, 2): (61, 12, 4, 0), (REF, 3): (61, 12, 4, 0),
+        (HOISTED, 0): (3, 0, 0, 2), (HOISTED, 1): (3, 0, 0, 2), (HOISTED, 2): (4, 0, 0, 2),
+        (HOISTED, 3): (4, 0, 0, 2),
+    }
+    for c in range(4):
+        rows = np.flatnonzero(case == c)
+        assert len(rows) > 50, c
+        for policy in (REF, HOISTED):
+            seen = {tuple(mh.count(policy, 1, X[i])[k] for k in ("div", "div2", "sqrt", "rsqrt")) for i in rows}
+            assert seen == {want[(policy, c)]}, (policy, c, seen)
 
 
 def test_hoisted_flux_equals_reference_order(mh):
