@@ -62,6 +62,8 @@ inline Num operator/(Num a, Num b)
     ++(b.v == 2.0 ? g_counts.div2 : g_counts.div);
     return Num(a.v / b.v);
 }
+inline Num &operator+=(Num &a, Num b) { return a = a + b; }
+inline Num &operator-=(Num &a, Num b) { return a = a - b; }
 inline bool operator<(Num a, Num b) { ++g_counts.cmp; return a.v < b.v; }
 inline bool operator>(Num a, Num b) { ++g_counts.cmp; return a.v > b.v; }
 inline bool operator<=(Num a, Num b) { ++g_counts.cmp; return a.v <= b.v; }
@@ -347,7 +349,9 @@ int mh_slope_vjp(long n, const double *in, const double *w, const double *k4, do
 // Operations of one evaluation for policy 0 = RefOrder or 1 = Hoisted:
 // what = 0 the GRP alone (face states in, 16 doubles as for mh_grp), 1 the
 // whole interface flux (cells and slopes in, as for mh_flux: face states,
-// GRP, midpoint flux).  counts: additions and subtractions,
+// GRP, midpoint flux), 2 the four limited slopes of a cell (12 doubles as for
+// mh_slope), 3 the conservative update (12 doubles as for mh_update; policy
+// 2 = HoistedCompensated counts the compensated one).  counts: additions and subtractions,
 // multiplications, divisions (by a variable), divisions by the constant 2,
 // square roots, reciprocal square roots, fused multiply-adds, comparisons.  Constant operands formed once per sweep
 // (SweepConsts) are not counted.
@@ -365,6 +369,14 @@ int mh_count(int policy, int what, const double *in, const double *k4, long *cou
         RefOrder::interface_flux(L, R, sL, sR, K);
     else if (policy == 1 && what == 1)
         Hoisted::interface_flux(L, R, sL, sR, K);
+    else if (what == 2 && policy <= 1)
+        policy == 0 ? RefOrder::slope(L, R, sL, K) : Hoisted::slope(L, R, sL, K);
+    else if (what == 3 && policy == 0)
+        RefOrder::update(L, R, sL, K);
+    else if (what == 3 && policy == 1)
+        Hoisted::update(L, R, sL, K);
+    else if (what == 3 && policy == 2)
+        HoistedCompensated::update(L, R, sL, K);
     else
         return 1;
     const opcount::Counts &c = opcount::g_counts;

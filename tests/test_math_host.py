@@ -159,6 +159,24 @@ def test_divisions_and_square_roots_per_interface(mh):
             assert seen == {want[(policy, c)]}, (policy, c, seen)
 
 
+def test_operations_per_cell_and_sweep(mh):
+    """A cell's share of one sweep: one interface flux, four limited slopes,
+    one update.  The shared-reciprocal slopes need no division and the
+    update one (the reference's five); the compensated update adds
+    error-free sums and products but no division."""
+    rng = np.random.default_rng(2)
+    n = 500
+    M = np.concatenate([cells(rng, n), cells(rng, n), cells(rng, n)], 1)
+    X = update_inputs(3, n)
+    pad = lambda x: np.pad(x, (0, 16 - len(x)))  # noqa: E731
+    for i in range(n):
+        s0, s1 = mh.count(REF, 2, pad(M[i])), mh.count(HOISTED, 2, pad(M[i]))
+        assert s0["div"] == s1["div"] == 0 and s1["mul"] <= s0["mul"]
+        u0, u1, u2 = (mh.count(p, 3, pad(X[i])) for p in (REF, HOISTED, COMPENSATED))
+        assert (u0["div"], u1["div"], u2["div"]) == (5, 1, 1)
+        assert u2["fma"] == 11  # the residuals of the two-products
+
+
 def test_hoisted_flux_equals_reference_order(mh):
     _, _, X = interfaces(2)
     F0 = mh("mh_flux", REF, 64, X)
