@@ -467,7 +467,7 @@ __device__ __forceinline__ Cell<Real> after_rows(const GhostArgs<Real> &a, int i
 template <typename Real>
 __device__ __forceinline__ Cell<Real> col_rule(const GhostArgs<Real> &a, int i, int j, double t)
 {
-    const int nx = a.nx, ny = a.ny;
+    const int nx = a.nx;
     const bool left = i < 2;
     switch (a.strategy) {
     case OUTFLOW:

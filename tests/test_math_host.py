@@ -115,6 +115,30 @@ def normwise(A, B):
     return (np.abs(A - B) / (np.abs(B) + np.median(np.abs(B), 0))).max(0)
 
 
+def test_reference_order_equals_the_oracle(mh, oracle):
+    """The host build of RefOrder (what the contraction-free GPU build runs)
+    against the oracle's C restatement (oracle/fvm2d_oracle.c, pinned to the
+    reference): GRP and slopes bit for bit, so the comparisons of the other
+    policies with RefOrder are comparisons with the pinned oracle."""
+    _, _, X = interfaces(7, 2000)
+    W = mh("mh_grp", REF, 64, X)
+    dp = ctypes.POINTER(ctypes.c_double)
+    for i in range(len(X)):
+        x = [np.ascontiguousarray(X[i, 4 * q:4 * q + 4]) for q in range(4)]
+        w, wt = np.zeros(5), np.zeros(5)
+        oracle.lib.orc_grp(*[a.ctypes.data_as(dp) for a in x], GAMMA, w.ctypes.data_as(dp), wt.ctypes.data_as(dp))
+        assert np.array_equal(W[i], np.concatenate([w, wt]), equal_nan=True), i
+    rng = np.random.default_rng(8)
+    C = np.concatenate([cells(rng, 2000), cells(rng, 2000), cells(rng, 2000)], 1)
+    S = mh("mh_slope", REF, 64, C)
+    for i in range(len(C)):
+        m, c, p = (np.ascontiguousarray(C[i, 4 * q:4 * q + 4]) for q in range(3))
+        s = np.zeros(4)
+        oracle.lib.orc_slope(m.ctypes.data_as(dp), c.ctypes.data_as(dp), p.ctypes.data_as(dp), H, ALPHA,
+                             s.ctypes.data_as(dp))
+        assert np.array_equal(S[i], s), i
+
+
 def test_hoisted_grp_equals_reference_order_in_every_wave_case(mh):
     L, R, X = interfaces(1)
     W0 = mh("mh_grp", REF, 64, X)
