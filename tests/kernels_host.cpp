@@ -1,19 +1,63 @@
-// kernels_host.cpp -- the parts of the sweep kernels' device code that run
-// one thread per cell with no exchange between threads -- the ghost-ring
-// rules (ghost_cell), the step-size plan (plan_step) and the wave speed --
-// compiled for the host with g++ from 2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh,
-// so that the CPU tests can compare them with the oracle on every preset and
-// slab row frame.  tests/test_kernels_host.py builds it and calls it through
-// ctypes.
+// kernels_host.cpp -- the device code of the step's kernels compiled for the
+// host with g++ from 2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh, so that the CPU
+// tests can compare it with the oracle without a GPU: the ghost-ring rules
+// (ghost_cell), the step-size plan (plan_step), the wave speed, and the sweep
+// work items themselves (x_item, y_item) with the kernels' item numbering.
+// tests/test_kernels_host.py builds it and calls it through ctypes.
 //
-// The rest of fvm2d_kernels.cuh uses warp, block and atomic intrinsics that
-// exist only in device code; they are declared below so that the header
-// compiles, and nothing called here reaches them.
+// An x-sweep work item is warp-cooperative: its lanes pass slopes and fluxes
+// to their neighbours with warp shuffles.  Here a warp is 32 host threads
+// running the same item sequence; a shuffle is a barrier-separated exchange
+// through a per-lane slot.  The block-level reductions and atomics of the
+// kernels themselves are declared so that the header compiles; nothing called
+// here reaches them.
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
+
+namespace warp_emu {
+constexpr int kLanes = 32;
+thread_local int lane_id = 0;
+struct Barrier {
+    std::mutex m;
+    std::condition_variable cv;
+    int count = 0, gen = 0;
+    void wait()
+    {
+        std::unique_lock<std::mutex> l(m);
+        const int g = gen;
+        if (++count == kLanes) {
+            count = 0;
+            ++gen;
+            cv.notify_all();
+        } else {
+            cv.wait(l, [&] { return gen != g; });
+        }
+    }
+};
+static Barrier bar;
+static unsigned char slot[kLanes][16];
+
+// value of lane (lane_id + delta), or the caller's own where that lane is
+// outside the warp, as the hardware shuffles do
+template <typename T>
+T exchange(T v, int delta)
+{
+    static_assert(sizeof(T) <= sizeof(slot[0]), "shuffle operand too wide");
+    std::memcpy(slot[lane_id], &v, sizeof(T));
+    bar.wait();
+    T r = v;
+    const int src = lane_id + delta;
+    if (src >= 0 && src < kLanes) std::memcpy(&r, slot[src], sizeof(T));
+    bar.wait();
+    return r;
+}
+} // namespace warp_emu
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
@@ -22,9 +66,9 @@ static dim3 blockDim, gridDim;
 template <typename T>
 static inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
 template <typename T>
-static inline T __shfl_down_sync(unsigned, T v, int) { return v; }
+static inline T __shfl_down_sync(unsigned, T v, int d) { return warp_emu::exchange(v, d); }
 template <typename T>
-static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
+static inline T __shfl_up_sync(unsigned, T v, int d) { return warp_emu::exchange(v, -d); }
 template <typename T>
 static inline T __shfl_sync(unsigned, T v, int) { return v; }
 static inline void __syncthreads() {}
@@ -138,6 +182,76 @@ int kh_wave_speed(long n, const double *cells, double gamma, double *out)
         const double *c = cells + 4 * i;
         out[i] = wave_speed(c[0], c[1], c[2], c[3], gamma);
     }
+    return 0;
+}
+
+// One sweep of a (ny, nx, 4) state through the kernels' work items: dir 0
+// runs x_item over every (row, 30-cell segment) item with a 32-thread warp,
+// dir 1 runs y_item over every (32-column, T-interface segment) item, lane by
+// lane (y items exchange nothing).  final (x only): the final sweep, which
+// averages with `comb` (branch A) in place, as the kernel does: `out` starts
+// as `comb` and is both read and written.  policy 0 = RefOrder, 1 = Hoisted.
+// Cells the items do not write are left NaN in `out` (or `comb`'s values).
+int kh_sweep(int policy, int dir, int final, int T, const double *in, const double *comb, double *out, int nx,
+             int ny, double h, double dt, double alpha, double gamma)
+{
+    if (nx < 6 || ny < 6 || (dir == 1 && T < 3) || (final && dir != 0)) return 1;
+    const long long plane = (long long)nx * ny;
+    if (final && !comb) return 1;
+    std::vector<double> S(4 * plane), D(4 * plane, NAN);
+    for (long long c = 0; c < plane; ++c)
+        for (int f = 0; f < 4; ++f) {
+            S[f * plane + c] = in[4 * c + f];
+            if (final) D[f * plane + c] = comb[4 * c + f];
+        }
+    SweepArgs<double> a;
+    a.src = Field<double>{S.data(), plane, nx};
+    a.dst = Field<double>{D.data(), plane, nx};
+    a.comb = a.dst;
+    a.flux = Field<double>{nullptr, plane, nx};
+    a.nx = nx;
+    a.ny = ny;
+    a.h = h;
+    a.rh = 1.0 / h;
+    a.alpha = alpha;
+    a.gamma = gamma;
+    a.ctl = nullptr;
+    const SweepConsts<double> K = sweep_consts(a, dt);
+    if (dir == 0) {
+        const int nseg = (nx - 4 + kXCells - 1) / kXCells;
+        const long long nwork = (long long)nseg * ny;
+        auto lane_run = [&](int lane) {
+            warp_emu::lane_id = lane;
+            double vmax = 0.0;
+            int bad = 0;
+            for (long long w = 0; w < nwork; ++w) {
+                const int y = int(w / nseg), seg = int(w % nseg);
+                if (policy == 0 && final)
+                    x_item<double, RefOrder, true>(a, K, y, seg, nseg, lane, vmax, bad);
+                else if (policy == 0)
+                    x_item<double, RefOrder, false>(a, K, y, seg, nseg, lane, vmax, bad);
+                else if (final)
+                    x_item<double, Hoisted, true>(a, K, y, seg, nseg, lane, vmax, bad);
+                else
+                    x_item<double, Hoisted, false>(a, K, y, seg, nseg, lane, vmax, bad);
+            }
+        };
+        std::vector<std::thread> warp;
+        for (int lane = 0; lane < warp_emu::kLanes; ++lane) warp.emplace_back(lane_run, lane);
+        for (auto &th : warp) th.join();
+    } else {
+        const int ncw = (nx + 31) / 32, nseg = y_segments(ny, T);
+        for (int seg = 0; seg < nseg; ++seg)
+            for (int cw = 0; cw < ncw; ++cw)
+                for (int lane = 0; lane < 32; ++lane) {
+                    if (policy == 0)
+                        y_item<double, RefOrder>(a, K, seg, nseg, cw, lane, T);
+                    else
+                        y_item<double, Hoisted>(a, K, seg, nseg, cw, lane, T);
+                }
+    }
+    for (long long c = 0; c < plane; ++c)
+        for (int f = 0; f < 4; ++f) out[4 * c + f] = D[f * plane + c];
     return 0;
 }
 

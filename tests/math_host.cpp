@@ -44,7 +44,8 @@ static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 // divisions and square roots each policy spends per interface.
 namespace opcount {
 struct Counts {
-    long add, mul, div, div2, sqrt, rsqrt, fma, cmp;  // div2: divisions by the constant 2 (a compiler makes them products)
+    // div2: divisions by the constant 2, which a compiler turns into products
+    long add, mul, div, div2, sqrt, rsqrt, fma, cmp;
 };
 static Counts g_counts;
 struct Num {

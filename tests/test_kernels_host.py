@@ -1,8 +1,16 @@
-"""The per-cell device code of the step that runs without exchanges between
-threads -- the ghost-ring rules (ghost_cell), the step-size plan
-(plan_step) and the wave speed -- compiled for the host from
-2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh (tests/kernels_host.cpp) and
-compared with the oracle bit for bit, without a GPU:
+"""The device code of the step's kernels -- the sweep work items (x_item
+with its lanes' shuffles run by a 32-thread host warp, y_item), the
+ghost-ring rules (ghost_cell), the step-size plan (plan_step) and the wave
+speed -- compiled for the host from 2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh
+(tests/kernels_host.cpp) and compared with the oracle bit for bit, without a
+GPU:
+
+* x and y sweeps through the kernels' own work items and item numbering
+  (30-cell row segments; 32-column segments of T interfaces for every T the
+  kernels choose), the final x-sweep averaging in place, and a whole step
+  composed as the kernels run it, in the reference's operation order
+  (RefOrder, what the contraction-free build runs); the shared-reciprocal
+  items within rounding;
 
 * the ghost fill on all seven presets, odd and even sizes, several times
   (the double-Mach shock moves with t), and the ring's wave-speed maximum;
@@ -28,8 +36,8 @@ def kh(tmp_path_factory):
     if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INC, "cuda_runtime.h")):
         pytest.skip("needs g++ and the CUDA headers")
     so = str(tmp_path_factory.mktemp("kernels_host") / "libkernels_host.so")
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I", CUDA_INC,
-                    os.path.join(HERE, "kernels_host.cpp"), "-o", so], check=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-pthread",
+                    "-I", CUDA_INC, os.path.join(HERE, "kernels_host.cpp"), "-o", so], check=True)
     lib = ctypes.CDLL(so)
     lib.kh_ghost.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -38,7 +46,27 @@ def kh(tmp_path_factory):
                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                             ctypes.c_void_p, ctypes.c_void_p]
     lib.kh_wave_speed.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
+    lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     return lib
+
+
+REF, HOISTED = 0, 1
+ALPHA, GAMMA = 1.9, 1.4
+
+
+def sweep(kh, policy, direction, U, h, dt, T=16, comb=None):
+    """direction 0: x-sweep items, 1: y-sweep items of T interfaces; comb:
+    the final x-sweep, averaging with comb in place."""
+    U = np.ascontiguousarray(U[..., :4], dtype=np.float64)
+    ny, nx = U.shape[:2]
+    out = np.empty_like(U)
+    cb = None if comb is None else np.ascontiguousarray(comb[..., :4], dtype=np.float64)
+    assert kh.kh_sweep(policy, direction, int(comb is not None), T, U.ctypes.data,
+                       None if cb is None else cb.ctypes.data, out.ctypes.data, nx, ny, h, dt, ALPHA, GAMMA) == 0
+    return out
+
+
+SWEEP_SIZES = [(48, 32), (37, 29), (33, 7), (6, 6), (70, 12)]
 
 
 def ghost(kh, U, strategy, t, row0=0, gny=None, top=True, bottom=True, gamma=1.4):
@@ -55,6 +83,52 @@ def ring_mask(ny, nx):
     m[:2] = m[-2:] = True
     m[:, :2] = m[:, -2:] = True
     return m
+
+
+def sweep_case(pkg, oracle, nx, ny, seed):
+    U = oracle.ghost(pkg.scenarios.seeded_four_quadrant(nx, ny, seed), 0)
+    width, height = 1.0, 1.1
+    dt = 0.3 * min(width / nx, height / ny) / oracle.max_speed(U)
+    return U, width, height, dt
+
+
+@pytest.mark.parametrize("nx,ny", SWEEP_SIZES)
+def test_sweep_items_equal_the_oracle_sweeps(kh, oracle, pkg, nx, ny):
+    U, width, height, dt = sweep_case(pkg, oracle, nx, ny, 3)
+    X = sweep(kh, REF, 0, U, width / nx, dt)
+    assert np.array_equal(X, oracle.sweep_x(U, width, dt))  # every cell written, bit for bit
+    RY = oracle.sweep_y(U, height, dt)
+    for T in (8, 16, 32, 64, 4):  # the kernels choose 64, 32, 16 or 8; 4 for short segments
+        assert np.array_equal(sweep(kh, REF, 1, U, height / ny, dt, T), RY), T
+
+
+@pytest.mark.parametrize("nx,ny", SWEEP_SIZES[:3])
+def test_hoisted_sweep_items_agree_to_rounding(kh, oracle, pkg, nx, ny):
+    U, width, height, dt = sweep_case(pkg, oracle, nx, ny, 4)
+    cases = ((0, oracle.sweep_x(U, width, dt), width / nx), (1, oracle.sweep_y(U, height, dt), height / ny))
+    for direction, R, h in cases:
+        H = sweep(kh, HOISTED, direction, U, h, dt)
+        rel = np.abs(H - R).max(axis=(0, 1)) / np.abs(R).max(axis=(0, 1))
+        assert rel.max() <= 1e-13, (direction, rel)  # measured 1.5e-16
+
+
+@pytest.mark.parametrize("strategy", [0, 4, 5])
+def test_one_step_composed_from_the_kernels_items(kh, oracle, pkg, strategy):
+    """The step as the kernels run it: X(U) -> A, Y(U) -> B, Y(A) -> U, the
+    final sweep X(B) averaged with U in place, then the ghost fill at the
+    advanced time; against the oracle's step."""
+    nx, ny = 45, 31
+    U = oracle.ghost(pkg.scenarios.seeded_four_quadrant(nx, ny, 12 + strategy), strategy)
+    kw = dict(width=1.0, height=0.8, cfl=0.45, alpha=ALPHA, gamma=GAMMA, t_end=1.0, strategy=strategy)
+    for _ in range(3):
+        R, t1, dt = oracle.step(U, t=0.0, **kw)
+        A = sweep(kh, REF, 0, U, kw["width"] / nx, dt)
+        B = sweep(kh, REF, 1, U, kw["height"] / ny, dt, T=8)
+        V = sweep(kh, REF, 1, A, kw["height"] / ny, dt, T=8)
+        V = sweep(kh, REF, 0, B, kw["width"] / nx, dt, comb=V)
+        V, _ = ghost(kh, V, strategy, t1)
+        assert np.array_equal(V, R)
+        U = R
 
 
 @pytest.mark.parametrize("strategy", range(7))
