@@ -4,3 +4,4 @@
 #define FVM2D_VARIANT adj32
 #define FVM2D_REAL float
 #include "fvm2d_adjoint.inc"
+#include "fvm2d_adjoint_launch.inc"

@@ -1,37 +1,50 @@
 // kernels_host.cpp -- the device code of the step's kernels compiled for the
-// host with g++ from 2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh, so that the CPU
-// tests can compare it with the oracle without a GPU: the ghost-ring rules
-// (ghost_cell), the step-size plan (plan_step), the wave speed, and the sweep
-// work items themselves (x_item, y_item) with the kernels' item numbering.
-// tests/test_kernels_host.py builds it and calls it through ctypes.
+// host with g++ from 2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh and
+// fvm2d_adjoint.inc, so that the CPU tests can compare it with the oracle
+// and with itself without a GPU: the ghost-ring rules (ghost_cell), the
+// step-size plan (plan_step), the wave speed, the sweep work items (x_item,
+// y_item) with the kernels' item numbering, and the adjoint step's kernels
+// (adjoint_x_kernel, adjoint_y_kernel, the ghost transposes) against a
+// dual-number tangent of the forward items.  tests/test_kernels_host.py
+// builds it and calls it through ctypes.
 //
-// An x-sweep work item is warp-cooperative: its lanes pass slopes and fluxes
-// to their neighbours with warp shuffles.  Here a warp is 32 host threads
-// running the same item sequence; a shuffle is a barrier-separated exchange
-// through a per-lane slot.  The block-level reductions and atomics of the
-// kernels themselves are declared so that the header compiles; nothing called
+// Launches are emulated block by block.  Kernels with warp shuffles or block
+// barriers run one host thread per CUDA thread: a shuffle is an exchange
+// through per-lane slots between two barriers of the warp's 32 threads,
+// __syncthreads a barrier of the block's threads, and __shared__ arrays are
+// static (one block runs at a time).  Kernels with neither run their threads
+// one after another.  The block-level reductions and atomics of the forward
+// kernels themselves are declared so that the headers compile; nothing called
 // here reaches them.
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
 
-namespace warp_emu {
-constexpr int kLanes = 32;
-thread_local int lane_id = 0;
+#undef __shared__
+#define __shared__ static
+
+static thread_local uint3 threadIdx;
+static uint3 blockIdx;
+static dim3 blockDim, gridDim;
+
+namespace emu {
+constexpr int kLanes = 32, kMaxWarps = 32;
+
 struct Barrier {
     std::mutex m;
     std::condition_variable cv;
-    int count = 0, gen = 0;
+    int count = 0, gen = 0, n = kLanes;
     void wait()
     {
         std::unique_lock<std::mutex> l(m);
         const int g = gen;
-        if (++count == kLanes) {
+        if (++count == n) {
             count = 0;
             ++gen;
             cv.notify_all();
@@ -40,38 +53,67 @@ struct Barrier {
         }
     }
 };
-static Barrier bar;
-static unsigned char slot[kLanes][16];
+static Barrier warp_bar[kMaxWarps];
+static Barrier block_bar;
+static unsigned char slot[kMaxWarps][kLanes][16];
 
-// value of lane (lane_id + delta), or the caller's own where that lane is
-// outside the warp, as the hardware shuffles do
+inline int flat_thread() { return int(threadIdx.x + threadIdx.y * blockDim.x); }
+
+// value of lane (lane + delta) of the caller's warp, or the caller's own
+// where that lane is outside the warp, as the hardware shuffles do
 template <typename T>
 T exchange(T v, int delta)
 {
-    static_assert(sizeof(T) <= sizeof(slot[0]), "shuffle operand too wide");
-    std::memcpy(slot[lane_id], &v, sizeof(T));
-    bar.wait();
+    static_assert(sizeof(T) <= sizeof(slot[0][0]), "shuffle operand too wide");
+    const int f = flat_thread(), w = f / kLanes, lane = f % kLanes;
+    std::memcpy(slot[w][lane], &v, sizeof(T));
+    warp_bar[w].wait();
     T r = v;
-    const int src = lane_id + delta;
-    if (src >= 0 && src < kLanes) std::memcpy(&r, slot[src], sizeof(T));
-    bar.wait();
+    const int src = lane + delta;
+    if (src >= 0 && src < kLanes) std::memcpy(&r, slot[w][src], sizeof(T));
+    warp_bar[w].wait();
     return r;
 }
-} // namespace warp_emu
+
+// Runs `body` as the kernel body of every thread of every block of the grid:
+// `threaded` for kernels that shuffle or wait at block barriers (whole warps
+// of threads), else thread after thread.
+template <class F>
+void launch(dim3 grid, dim3 block, bool threaded, F body)
+{
+    gridDim = grid;
+    blockDim = block;
+    const int nt = int(block.x * block.y);
+    block_bar.n = nt;
+    for (unsigned by = 0; by < grid.y; ++by)
+        for (unsigned bx = 0; bx < grid.x; ++bx) {
+            blockIdx = make_uint3(bx, by, 0);
+            auto run = [&](int t) {
+                threadIdx = make_uint3(unsigned(t) % block.x, unsigned(t) / block.x, 0);
+                body();
+            };
+            if (threaded) {
+                std::vector<std::thread> th;
+                for (int t = 0; t < nt; ++t) th.emplace_back(run, t);
+                for (auto &x : th) x.join();
+            } else {
+                for (int t = 0; t < nt; ++t) run(t);
+            }
+        }
+}
+} // namespace emu
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
-static uint3 threadIdx, blockIdx;
-static dim3 blockDim, gridDim;
 template <typename T>
 static inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
 template <typename T>
-static inline T __shfl_down_sync(unsigned, T v, int d) { return warp_emu::exchange(v, d); }
+static inline T __shfl_down_sync(unsigned, T v, int d) { return emu::exchange(v, d); }
 template <typename T>
-static inline T __shfl_up_sync(unsigned, T v, int d) { return warp_emu::exchange(v, -d); }
+static inline T __shfl_up_sync(unsigned, T v, int d) { return emu::exchange(v, -d); }
 template <typename T>
 static inline T __shfl_sync(unsigned, T v, int) { return v; }
-static inline void __syncthreads() {}
+static inline void __syncthreads() { emu::block_bar.wait(); }
 static inline void __threadfence() {}
 static inline int __any_sync(unsigned, int p) { return p; }
 static inline long long __double_as_longlong(double x)
@@ -113,9 +155,149 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 #define __launch_bounds__(...)
 
 #define FVM2D_VARIANT host
+#define FVM2D_REAL double
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc"
 
 using namespace fvm2d::host;
+using fvm2d::ad::Dual;
+
+namespace {
+
+// Four planes of pitch nx for a (ny, nx) array.
+template <typename R>
+struct Planes {
+    int nx = 0, ny = 0;
+    long long plane = 0;
+    std::vector<R> v;
+    Planes() = default;
+    Planes(int nx_, int ny_) : nx(nx_), ny(ny_), plane((long long)nx_ * ny_), v(4 * plane, R(0.0)) {}
+    Field<R> field() { return Field<R>{v.data(), plane, nx}; }
+};
+
+template <typename R>
+SweepArgs<R> sweep_args(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double alpha, double gamma)
+{
+    SweepArgs<R> a;
+    a.src = src.field();
+    a.dst = dst.field();
+    a.comb = a.dst;
+    a.flux = flux ? flux->field() : Field<R>{nullptr, src.plane, src.nx};
+    a.nx = src.nx;
+    a.ny = src.ny;
+    a.h = h;
+    a.rh = 1.0 / h;
+    a.alpha = alpha;
+    a.gamma = gamma;
+    a.ctl = nullptr;
+    return a;
+}
+
+// x-sweep src -> dst through x_item on one emulated warp (FINAL: dst holds
+// branch A and is averaged in place); TAPE stores the interface fluxes.
+template <typename R, bool FINAL, bool TAPE>
+void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma)
+{
+    const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
+    const SweepConsts<R> K = sweep_consts(a, dt);
+    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
+    const long long nwork = (long long)nseg * a.ny;
+    emu::launch(dim3(1), dim3(32), true, [&] {
+        double vmax = 0.0;
+        int bad = 0;
+        for (long long w = 0; w < nwork; ++w)
+            x_item<R, Hoisted, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
+    });
+}
+
+// y-sweep src -> dst through y_item, segments of T interfaces.
+template <typename R, bool TAPE>
+void y_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma, int T)
+{
+    const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
+    const SweepConsts<R> K = sweep_consts(a, dt);
+    const int ncw = (a.nx + 31) / 32, nseg = y_segments(a.ny, T);
+    for (int seg = 0; seg < nseg; ++seg)
+        for (int cw = 0; cw < ncw; ++cw)
+            for (int lane = 0; lane < 32; ++lane) y_item<R, Hoisted, TAPE>(a, K, seg, nseg, cw, lane, T);
+}
+
+// One split step U -> out of the shared-reciprocal build, in the kernels'
+// order (X(U) -> A, Y(U) -> B, Y(A) -> out, X(B) averaged with out, ghost
+// fill of out at t + dt); TAPE keeps A, B and the four sweeps' fluxes.
+template <typename R, bool TAPE>
+void forward_step(Planes<R> &U, Planes<R> &A, Planes<R> &B, Planes<R> &out, Planes<R> *flux, int strategy, double t,
+                  double dt, double hx, double hy, double alpha, double gamma, int T)
+{
+    x_sweep<R, false, TAPE>(U, A, TAPE ? &flux[0] : nullptr, hx, dt, alpha, gamma);
+    y_sweep<R, TAPE>(U, B, TAPE ? &flux[1] : nullptr, hy, dt, alpha, gamma, T);
+    y_sweep<R, TAPE>(A, out, TAPE ? &flux[2] : nullptr, hy, dt, alpha, gamma, T);
+    x_sweep<R, true, TAPE>(B, out, TAPE ? &flux[3] : nullptr, hx, dt, alpha, gamma);
+    GhostArgs<R> g;
+    g.U = out.field();
+    g.nx = U.nx;
+    g.ny = U.ny;
+    g.strategy = strategy;
+    g.gamma = gamma;
+    g.ctl = nullptr;
+    g.plan = fvm2d::PlanParams{};
+    g.row0 = 0;
+    g.gny = U.ny;
+    g.fill_top = g.fill_bottom = 1;
+    for (int k = 0; k < 4 * U.nx + 4 * (U.ny - 4); ++k) ghost_cell(g, k, t + dt);
+}
+
+template <typename R>
+void cells_to(Planes<R> &P, const double *cells, const double *tangent)
+{
+    for (long long c = 0; c < P.plane; ++c)
+        for (int f = 0; f < 4; ++f) {
+            if constexpr (std::is_same_v<R, Dual>)
+                P.v[f * P.plane + c] = R(cells[4 * c + f], tangent[4 * c + f]);
+            else
+                P.v[f * P.plane + c] = R(cells[4 * c + f]);
+        }
+}
+
+// The sweep transposes' constants, formed as the adjoint step's launcher
+// forms them (the forward's sweep_consts: lambda = dt / h).
+SweepConsts<A> adjoint_consts(double h, double dt, double alpha, double gamma)
+{
+    SweepConsts<A> K;
+    K.h = h;
+    K.rh = 1.0 / h;
+    K.alpha = alpha;
+    K.g = gamma;
+    K.k = dt;
+    K.lambda = dt / h;
+    K.igm1 = 1.0 / (gamma - 1.0);
+    K.kappa = (gamma + 1.0) / 2.0;
+    return K;
+}
+
+// out = (d sweep_dir at U)^T ub (+ addend), with the grids the launcher uses
+// (adjoint_x_kernel grid-strides, here one block of 128 threads).
+void transpose(int dir, Planes<double> &U, Planes<double> &F, Planes<double> &ub, Planes<double> &out,
+               Planes<double> *addend, double h, double dt, double alpha, double gamma)
+{
+    SweepT g;
+    g.U = U.field();
+    g.F = F.field();
+    g.ub = ub.field();
+    g.out = out.field();
+    g.addend = addend ? addend->field() : Field<double>{nullptr, U.plane, U.nx};
+    g.nx = U.nx;
+    g.ny = U.ny;
+    g.K = adjoint_consts(h, dt, alpha, gamma);
+    if (dir == 0)
+        emu::launch(dim3(1), dim3(ANT), true, [&] { adjoint_x_kernel(g); });
+    else
+        emu::launch(dim3((U.nx + kTileCols - 1) / kTileCols, (U.ny + kLineOut - 1) / kLineOut), dim3(ANT), true,
+                    [&] { adjoint_y_kernel(g); });
+}
+
+} // namespace
 using fvm2d::PlanParams;
 using fvm2d::StepControl;
 
@@ -220,8 +402,8 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
     if (dir == 0) {
         const int nseg = (nx - 4 + kXCells - 1) / kXCells;
         const long long nwork = (long long)nseg * ny;
-        auto lane_run = [&](int lane) {
-            warp_emu::lane_id = lane;
+        emu::launch(dim3(1), dim3(32), true, [&] {
+            const int lane = int(threadIdx.x);
             double vmax = 0.0;
             int bad = 0;
             for (long long w = 0; w < nwork; ++w) {
@@ -235,10 +417,7 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
                 else
                     x_item<double, Hoisted, false>(a, K, y, seg, nseg, lane, vmax, bad);
             }
-        };
-        std::vector<std::thread> warp;
-        for (int lane = 0; lane < warp_emu::kLanes; ++lane) warp.emplace_back(lane_run, lane);
-        for (auto &th : warp) th.join();
+        });
     } else {
         const int ncw = (nx + 31) / 32, nseg = y_segments(ny, T);
         for (int seg = 0; seg < nseg; ++seg)
@@ -252,6 +431,55 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
     }
     for (long long c = 0; c < plane; ++c)
         for (int f = 0; f < 4; ++f) out[4 * c + f] = D[f * plane + c];
+    return 0;
+}
+
+// Tangent of one split step of the shared-reciprocal build at a (ny, nx, 4)
+// state `cells` along `dir`, from the forward work items run on dual numbers:
+// out = the step's result, out_t = its tangent.  T: y segment length.
+int kh_step_jvp(const double *cells, const double *dir, int nx, int ny, int strategy, double t, double dt,
+                double width, double height, double alpha, double gamma, int T, double *out, double *out_t)
+{
+    if (nx < 6 || ny < 6) return 1;
+    Planes<Dual> U(nx, ny), A(nx, ny), B(nx, ny), V(nx, ny);
+    cells_to(U, cells, dir);
+    forward_step<Dual, false>(U, A, B, V, nullptr, strategy, t, dt, width / nx, height / ny, alpha, gamma, T);
+    for (long long c = 0; c < V.plane; ++c)
+        for (int f = 0; f < 4; ++f) {
+            out[4 * c + f] = V.v[f * V.plane + c].v;
+            out_t[4 * c + f] = V.v[f * V.plane + c].d;
+        }
+    return 0;
+}
+
+// Adjoint of the same step: the taped forward on doubles, then the adjoint
+// step's kernels in the launcher's order (ghost transpose into H, then
+// Y^T(A1) and X^T(U) for branch A, X^T(B1) and Y^T(U) for branch B, summed):
+// in_b = (d step at cells)^T out_b.
+int kh_step_vjp(const double *cells, const double *out_b, int nx, int ny, int strategy, double t, double dt,
+                double width, double height, double alpha, double gamma, int T, double *in_b)
+{
+    if (nx < 6 || ny < 6) return 1;
+    const double hx = width / nx, hy = height / ny;
+    Planes<double> U(nx, ny), A1(nx, ny), B1(nx, ny), V(nx, ny);
+    Planes<double> flux[4] = {Planes<double>(nx, ny), Planes<double>(nx, ny), Planes<double>(nx, ny),
+                              Planes<double>(nx, ny)};
+    cells_to(U, cells, nullptr);
+    forward_step<double, true>(U, A1, B1, V, flux, strategy, t, dt, hx, hy, alpha, gamma, T);
+    Planes<double> lb(nx, ny), H(nx, ny), T1(nx, ny), T2(nx, ny), out(nx, ny);
+    cells_to(lb, out_b, nullptr);
+    const GhostGeom gg{nx, ny, strategy};
+    Field<double> lbf = lb.field(), Hf = H.field();
+    emu::launch(dim3((nx + 31) / 32, (ny + 7) / 8), dim3(32, 8), false,
+                [&] { ghost_adjoint_copy(lbf, Hf, gg, 0.5); });
+    const int ring = 4 * nx + 4 * (ny - 4);
+    emu::launch(dim3((ring + 255) / 256), dim3(256), false, [&] { ghost_adjoint_scatter(lbf, Hf, gg, 0.5); });
+    transpose(1, A1, flux[2], H, T1, nullptr, hy, dt, alpha, gamma);
+    transpose(0, U, flux[0], T1, T2, nullptr, hx, dt, alpha, gamma);
+    transpose(0, B1, flux[3], H, T1, nullptr, hx, dt, alpha, gamma);
+    transpose(1, U, flux[1], T1, out, &T2, hy, dt, alpha, gamma);
+    for (long long c = 0; c < out.plane; ++c)
+        for (int f = 0; f < 4; ++f) in_b[4 * c + f] = out.v[f * out.plane + c];
     return 0;
 }
 

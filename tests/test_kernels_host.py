@@ -17,7 +17,12 @@ GPU:
 * the same fill in the row frames of slabs (global row numbers for the jet
   rows and the shock, only the problem's own edges filled);
 * the step size and end-of-loop decision of the reference's rule
-  (src/wrappers.cuh:196-207, the oracle's orc_dt).
+  (src/wrappers.cuh:196-207, the oracle's orc_dt);
+* the adjoint step's own kernels (2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc:
+  the x and y sweep transposes, with the y tiles in shared memory and block
+  barriers, and the ghost-ring transposes) as the transpose of the
+  dual-number tangent of the forward work items, on every preset:
+  <J v, w> = <v, J^T w>.
 """
 import ctypes
 import os
@@ -47,6 +52,9 @@ def kh(tmp_path_factory):
                             ctypes.c_void_p, ctypes.c_void_p]
     lib.kh_wave_speed.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
     lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
+    step = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int]
+    lib.kh_step_jvp.argtypes = step + [ctypes.c_void_p] * 2
+    lib.kh_step_vjp.argtypes = step + [ctypes.c_void_p]
     return lib
 
 
@@ -211,3 +219,31 @@ def test_wave_speed_equals_the_oracle(kh, oracle, pkg):
     assert out.max() == oracle.max_speed(U)
     for row in (0, 57, 199):
         assert out.reshape(200, 300)[row].max() == oracle.max_speed(np.ascontiguousarray(U[row:row + 1]))
+
+
+@pytest.mark.parametrize("strategy", range(7))
+def test_adjoint_kernels_transpose_the_forward_items(kh, oracle, pkg, strategy):
+    """One step at a perturbed four-quadrant state (no cell pair exactly
+    equal, so no limiter or wave-case test sits on its switch): the tangent
+    J v from the forward items on dual numbers and the cotangent J^T w from
+    the adjoint kernels satisfy <J v, w> = <v, J^T w> to rounding; the
+    dual run's values are the step itself (checked against the oracle)."""
+    nx, ny, width, height, t = 37, 29, 1.0, 0.8, 0.01
+    rng = np.random.default_rng(strategy)
+    U = oracle.ghost(pkg.scenarios.seeded_four_quadrant(nx, ny, 40 + strategy), strategy)
+    U = U * (1 + 0.05 * rng.standard_normal(U.shape) * [1, 1, 0, 0]) + 0.05 * rng.standard_normal(U.shape) * [0, 0, 1, 1]
+    U = np.ascontiguousarray(U)
+    dt = 0.3 * min(width / nx, height / ny) / oracle.max_speed(U)
+    v = np.ascontiguousarray(rng.standard_normal(U.shape))
+    w = np.ascontiguousarray(rng.standard_normal(U.shape))
+    out, Jv, JTw = np.empty_like(U), np.empty_like(U), np.empty_like(U)
+    args = (nx, ny, strategy, t, dt, width, height, ALPHA, GAMMA, 8)
+    assert kh.kh_step_jvp(U.ctypes.data, v.ctypes.data, *args, out.ctypes.data, Jv.ctypes.data) == 0
+    assert kh.kh_step_vjp(U.ctypes.data, w.ctypes.data, *args, JTw.ctypes.data) == 0
+    # the value part: the shared-reciprocal step, against the oracle's sweeps and fill
+    A = oracle.sweep_y(oracle.sweep_x(U, width, dt), height, dt)
+    B = oracle.sweep_x(oracle.sweep_y(U, height, dt), width, dt)
+    R = oracle.ghost((A + B) * 0.5, strategy, t=t + dt, width=width, height=height)
+    assert np.abs(out - R).max() <= 1e-12 * np.abs(R).max()
+    a, b = np.sum(Jv * w), np.sum(v * JTw)
+    assert abs(a - b) <= 1e-13 * max(abs(a), abs(b)), (a, b)  # measured <= 1.6e-15
