@@ -105,6 +105,13 @@ void launch(dim3 grid, dim3 block, bool threaded, F body)
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+// sm_100's two-wide FP32 instructions: two correctly rounded operations
+static inline float2 __fadd2_rn(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+static inline float2 __fmul2_rn(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+static inline float2 __ffma2_rn(float2 a, float2 b, float2 c)
+{
+    return make_float2(std::fma(a.x, b.x, c.x), std::fma(a.y, b.y, c.y));
+}
 template <typename T>
 static inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
 template <typename T>
@@ -159,6 +166,7 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_kernels.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
 
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
@@ -196,7 +204,7 @@ SweepArgs<R> sweep_args(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double 
 
 // x-sweep src -> dst through x_item on one emulated warp (FINAL: dst holds
 // branch A and is averaged in place); TAPE stores the interface fluxes.
-template <typename R, bool FINAL, bool TAPE>
+template <typename R, bool FINAL, bool TAPE, class Phys = Hoisted>
 void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma)
 {
     const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
@@ -207,12 +215,12 @@ void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double d
         double vmax = 0.0;
         int bad = 0;
         for (long long w = 0; w < nwork; ++w)
-            x_item<R, Hoisted, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
+            x_item<R, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
     });
 }
 
 // y-sweep src -> dst through y_item, segments of T interfaces.
-template <typename R, bool TAPE>
+template <typename R, bool TAPE, class Phys = Hoisted>
 void y_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma, int T)
 {
     const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
@@ -220,7 +228,7 @@ void y_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double d
     const int ncw = (a.nx + 31) / 32, nseg = y_segments(a.ny, T);
     for (int seg = 0; seg < nseg; ++seg)
         for (int cw = 0; cw < ncw; ++cw)
-            for (int lane = 0; lane < 32; ++lane) y_item<R, Hoisted, TAPE>(a, K, seg, nseg, cw, lane, T);
+            for (int lane = 0; lane < 32; ++lane) y_item<R, Phys, TAPE>(a, K, seg, nseg, cw, lane, T);
 }
 
 // One split step U -> out of the shared-reciprocal build, in the kernels'
@@ -480,6 +488,27 @@ int kh_step_vjp(const double *cells, const double *out_b, int nx, int ny, int st
     transpose(1, U, flux[1], T1, out, &T2, hy, dt, alpha, gamma);
     for (long long c = 0; c < out.plane; ++c)
         for (int f = 0; f < 4; ++f) in_b[4 * c + f] = out.v[f * out.plane + c];
+    return 0;
+}
+
+// One sweep in the FP32 build's arithmetic (FP32 planes, PackedCompensated
+// physics, the float overloads of the limiter): dir 0 x, 1 y (T interfaces
+// per segment); final (x only) averages with comb in place.
+int kh_sweep32(int dir, int final, int T, const double *in, const double *comb, double *out, int nx, int ny,
+               double h, double dt, double alpha, double gamma)
+{
+    if (nx < 6 || ny < 6 || (dir == 1 && T < 3) || (final && (dir != 0 || !comb))) return 1;
+    Planes<float> S(nx, ny), D(nx, ny);
+    cells_to(S, in, nullptr);
+    if (final) cells_to(D, comb, nullptr);
+    if (dir == 0 && final)
+        x_sweep<float, true, false, PackedCompensated>(S, D, nullptr, h, dt, alpha, gamma);
+    else if (dir == 0)
+        x_sweep<float, false, false, PackedCompensated>(S, D, nullptr, h, dt, alpha, gamma);
+    else
+        y_sweep<float, false, PackedCompensated>(S, D, nullptr, h, dt, alpha, gamma, T);
+    for (long long c = 0; c < D.plane; ++c)
+        for (int f = 0; f < 4; ++f) out[4 * c + f] = double(D.v[f * D.plane + c]);
     return 0;
 }
 

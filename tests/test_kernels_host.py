@@ -10,7 +10,8 @@ GPU:
   kernels choose), the final x-sweep averaging in place, and a whole step
   composed as the kernels run it, in the reference's operation order
   (RefOrder, what the contraction-free build runs); the shared-reciprocal
-  items within rounding;
+  items within rounding, and the FP32 build's items (PackedCompensated,
+  32-bit plane offsets) within single-precision rounding;
 
 * the ghost fill on all seven presets, odd and even sizes, several times
   (the double-Mach shock moves with t), and the ring's wave-speed maximum;
@@ -53,6 +54,7 @@ def kh(tmp_path_factory):
     lib.kh_wave_speed.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
     lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     step = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int]
+    lib.kh_sweep32.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_step_jvp.argtypes = step + [ctypes.c_void_p] * 2
     lib.kh_step_vjp.argtypes = step + [ctypes.c_void_p]
     return lib
@@ -118,6 +120,34 @@ def test_hoisted_sweep_items_agree_to_rounding(kh, oracle, pkg, nx, ny):
         H = sweep(kh, HOISTED, direction, U, h, dt)
         rel = np.abs(H - R).max(axis=(0, 1)) / np.abs(R).max(axis=(0, 1))
         assert rel.max() <= 1e-13, (direction, rel)  # measured 1.5e-16
+
+
+def normwise(A, R):
+    return (np.abs(A - R) / (np.abs(R) + np.median(np.abs(R), axis=(0, 1)))).max()
+
+
+@pytest.mark.parametrize("nx,ny", SWEEP_SIZES[:4])
+def test_fp32_sweep_items_stay_within_single_precision(kh, oracle, pkg, nx, ny):
+    """The FP32 build's items on FP32 values against the oracle's FP64 sweeps
+    of the same values: about one FP32 rounding (measured 8.7e-8)."""
+    U, width, height, dt = sweep_case(pkg, oracle, nx, ny, 5)
+    U = np.ascontiguousarray(U.astype(np.float32).astype(np.float64))
+
+    def sweep32(direction, V, h, T=16, comb=None):
+        out = np.empty_like(V)
+        cb = None if comb is None else np.ascontiguousarray(comb)
+        assert kh.kh_sweep32(direction, int(comb is not None), T, V.ctypes.data,
+                             None if cb is None else cb.ctypes.data, out.ctypes.data, nx, ny, h, dt, ALPHA,
+                             GAMMA) == 0
+        return out
+
+    assert normwise(sweep32(0, U, width / nx), oracle.sweep_x(U, width, dt)) <= 5e-7
+    RY = oracle.sweep_y(U, height, dt)
+    for T in (8, 16, 32, 64):
+        assert normwise(sweep32(1, U, height / ny, T), RY) <= 5e-7, T
+    A = np.ascontiguousarray(RY.astype(np.float32).astype(np.float64))
+    F = sweep32(0, U, width / nx, comb=A)
+    assert normwise(F, (oracle.sweep_x(U, width, dt) + A) * 0.5) <= 5e-7
 
 
 @pytest.mark.parametrize("strategy", [0, 4, 5])
