@@ -3,21 +3,23 @@
 // fvm2d_adjoint.inc, so that the CPU tests can compare it with the oracle
 // and with itself without a GPU: the ghost-ring rules (ghost_cell), the
 // step-size plan (plan_step), the wave speed, the sweep work items (x_item,
-// y_item) with the kernels' item numbering, and the adjoint step's kernels
+// y_item) with the kernels' item numbering, the batched kernels
+// (fvm2d_batch.cuh) over several problems, and the adjoint step's kernels
 // (adjoint_x_kernel, adjoint_y_kernel, the ghost transposes) against a
 // dual-number tangent of the forward items.  tests/test_kernels_host.py
 // builds it and calls it through ctypes.
 //
 // Launches are emulated block by block.  Kernels with warp shuffles or block
 // barriers run one host thread per CUDA thread: a shuffle is an exchange
-// through per-lane slots between two barriers of the warp's 32 threads,
-// __syncthreads a barrier of the block's threads, and __shared__ arrays are
+// through per-lane slots between two barriers of the warp's 32 threads (a
+// butterfly shuffle and a vote likewise), __syncthreads a barrier of the
+// block's threads, atomics take a lock, and __shared__ arrays are
 // static (one block runs at a time).  Kernels with neither run their threads
 // one after another.  The block-level reductions and atomics of the forward
 // kernels themselves are declared so that the headers compile; nothing called
 // here reaches them.
+#include <atomic>
 #include <cmath>
-#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -36,20 +38,20 @@ static dim3 blockDim, gridDim;
 namespace emu {
 constexpr int kLanes = 32, kMaxWarps = 32;
 
+// Generation barrier of n threads; waiters yield rather than sleep (the
+// emulated warps run far more threads than cores, and a barrier releases
+// within microseconds).
 struct Barrier {
-    std::mutex m;
-    std::condition_variable cv;
-    int count = 0, gen = 0, n = kLanes;
+    std::atomic<int> count{0}, gen{0};
+    int n = kLanes;
     void wait()
     {
-        std::unique_lock<std::mutex> l(m);
-        const int g = gen;
-        if (++count == n) {
-            count = 0;
-            ++gen;
-            cv.notify_all();
+        const int g = gen.load(std::memory_order_acquire);
+        if (count.fetch_add(1, std::memory_order_acq_rel) == n - 1) {
+            count.store(0, std::memory_order_relaxed);
+            gen.fetch_add(1, std::memory_order_release);
         } else {
-            cv.wait(l, [&] { return gen != g; });
+            while (gen.load(std::memory_order_acquire) == g) std::this_thread::yield();
         }
     }
 };
@@ -74,6 +76,32 @@ T exchange(T v, int delta)
     warp_bar[w].wait();
     return r;
 }
+
+// lane ^ mask's value (butterfly shuffle)
+template <typename T>
+T exchange_xor(T v, int mask)
+{
+    const int lane = flat_thread() % kLanes;
+    return exchange(v, (lane ^ mask) - lane);
+}
+
+// warp vote: nonzero if any lane's predicate is
+inline int vote_any(int pred)
+{
+    const int f = flat_thread(), w = f / kLanes, lane = f % kLanes;
+    std::memcpy(slot[w][lane], &pred, sizeof pred);
+    warp_bar[w].wait();
+    int any = 0;
+    for (int l = 0; l < kLanes; ++l) {
+        int q;
+        std::memcpy(&q, slot[w][l], sizeof q);
+        any |= q != 0;
+    }
+    warp_bar[w].wait();
+    return any;
+}
+
+static std::mutex atomic_mutex;  // the atomics of threaded launches
 
 // Runs `body` as the kernel body of every thread of every block of the grid:
 // `threaded` for kernels that shuffle or wait at block barriers (whole warps
@@ -113,7 +141,7 @@ static inline float2 __ffma2_rn(float2 a, float2 b, float2 c)
     return make_float2(std::fma(a.x, b.x, c.x), std::fma(a.y, b.y, c.y));
 }
 template <typename T>
-static inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
+static inline T __shfl_xor_sync(unsigned, T v, int m) { return emu::exchange_xor(v, m); }
 template <typename T>
 static inline T __shfl_down_sync(unsigned, T v, int d) { return emu::exchange(v, d); }
 template <typename T>
@@ -122,7 +150,7 @@ template <typename T>
 static inline T __shfl_sync(unsigned, T v, int) { return v; }
 static inline void __syncthreads() { emu::block_bar.wait(); }
 static inline void __threadfence() {}
-static inline int __any_sync(unsigned, int p) { return p; }
+static inline int __any_sync(unsigned, int p) { return emu::vote_any(p); }
 static inline long long __double_as_longlong(double x)
 {
     long long r;
@@ -138,6 +166,7 @@ static inline double __longlong_as_double(long long x)
 template <typename T>
 static inline T atomicAdd(T *p, T v)
 {
+    std::lock_guard<std::mutex> g(emu::atomic_mutex);
     const T o = *p;
     *p = o + v;
     return o;
@@ -145,6 +174,7 @@ static inline T atomicAdd(T *p, T v)
 template <typename T>
 static inline T atomicMax(T *p, T v)
 {
+    std::lock_guard<std::mutex> g(emu::atomic_mutex);
     const T o = *p;
     if (v > o) *p = v;
     return o;
@@ -152,6 +182,7 @@ static inline T atomicMax(T *p, T v)
 template <typename T>
 static inline T atomicCAS(T *p, T c, T v)
 {
+    std::lock_guard<std::mutex> g(emu::atomic_mutex);
     const T o = *p;
     if (o == c) *p = v;
     return o;
@@ -167,6 +198,7 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh"
 
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
@@ -509,6 +541,109 @@ int kh_sweep32(int dir, int final, int T, const double *in, const double *comb, 
         y_sweep<float, false, PackedCompensated>(S, D, nullptr, h, dt, alpha, gamma, T);
     for (long long c = 0; c < D.plane; ++c)
         for (int f = 0; f < 4; ++f) out[4 * c + f] = double(D.v[f * D.plane + c]);
+    return 0;
+}
+
+// A batch of np problems solved by the batched kernels in the reference
+// order (RefOrder), launched as the batch runtime launches them: the initial
+// wave-speed kernel, then per step the x, y, y and final x sweeps over all
+// problems' items and the ghost kernel, until every problem's loop has ended
+// (or max_steps steps).  Problem p is nx[p] x ny[p] cells, `cells` the
+// problems' (ny, nx, 4) states one after another; params[7p..7p+6] = width,
+// height, t_end, cfl, alpha, gamma, strategy.  The descriptors are laid out
+// as the batch runtime lays them out (rows padded to 32, u/a/b buffers per
+// problem, prefix counts of items and blocks); grid_x, grid_y: blocks of the
+// sweep launches (chunks of items per warp).
+int kh_batch_solve(int np, const int *nx, const int *ny, const double *params, const double *cells, int T,
+                   int grid_x, int grid_y, int max_steps, double *out_cells, double *out_t, int *out_steps)
+{
+    constexpr int kSweepThreads = 128, kGhostThreads = 256, kInitThreads = 256;
+    std::vector<fvm2d::BatchProblem> P(np);
+    std::vector<long long> x0(np + 1, 0), y0(np + 1, 0), off(np + 1, 0);
+    std::vector<int> rb0(np + 1, 0), ib0(np + 1, 0);
+    for (int p = 0; p < np; ++p) {
+        if (nx[p] < 6 || ny[p] < 6) return 1;
+        fvm2d::BatchProblem &q = P[p];
+        std::memset(&q, 0, sizeof q);
+        const double *pr = params + 7 * p;
+        q.pitch = (nx[p] + 31) / 32 * 32;
+        q.plane = (long long)q.pitch * ny[p];
+        q.u = off[p];
+        q.a = off[p] + 4 * q.plane;
+        q.b = off[p] + 8 * q.plane;
+        off[p + 1] = off[p] + 12 * q.plane;
+        q.nx = nx[p];
+        q.ny = ny[p];
+        q.strategy = int(pr[6]);
+        q.hx = pr[0] / double(nx[p]);
+        q.hy = pr[1] / double(ny[p]);
+        q.rhx = 1.0 / q.hx;
+        q.rhy = 1.0 / q.hy;
+        q.alpha = pr[4];
+        q.gamma = pr[5];
+        q.plan.t_end = pr[2];
+        q.plan.cfl = pr[3];
+        q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
+        q.plan.fixed_dt = 0.0;
+        q.nsegx = (nx[p] - 4 + 29) / 30;
+        q.ncw = (nx[p] + 31) / 32;
+        q.T = T;
+        q.nsegy = y_segments(ny[p], T);
+        q.ring = 4 * nx[p] + 4 * (ny[p] - 4);
+        x0[p + 1] = x0[p] + (long long)q.nsegx * ny[p];
+        y0[p + 1] = y0[p] + (long long)q.ncw * q.nsegy;
+        rb0[p + 1] = rb0[p] + (q.ring + kGhostThreads - 1) / kGhostThreads;
+        const long long n = (long long)nx[p] * ny[p];
+        ib0[p + 1] = ib0[p] + int((n + fvm2d::kBatchInitCells - 1) / fvm2d::kBatchInitCells);
+    }
+    std::vector<double> base(off[np], 0.0);
+    std::vector<StepControl> ctl(np);
+    long long c0 = 0;
+    for (int p = 0; p < np; ++p) {
+        std::memset(&ctl[p], 0, sizeof(StepControl));
+        ctl[p].step_limit = max_steps;
+        for (int y = 0; y < ny[p]; ++y)
+            for (int x = 0; x < nx[p]; ++x)
+                for (int f = 0; f < 4; ++f)
+                    base[P[p].u + f * P[p].plane + (long long)y * P[p].pitch + x] =
+                        cells[c0 + 4 * ((long long)y * nx[p] + x) + f];
+        c0 += 4LL * nx[p] * ny[p];
+    }
+    BatchArgs<double> b;
+    b.base = base.data();
+    b.prob = P.data();
+    b.ctl = ctl.data();
+    b.x0 = x0.data();
+    b.y0 = y0.data();
+    b.rb0 = rb0.data();
+    b.ib0 = ib0.data();
+    b.np = np;
+    const long long xt = x0[np], yt = y0[np];
+    emu::launch(dim3(ib0[np]), dim3(kInitThreads), true, [&] { batch_init_kernel<double, kInitThreads>(b); });
+    for (int step = 0; step < max_steps; ++step) {
+        bool any = false;
+        for (int p = 0; p < np; ++p) any |= ctl[p].active != 0;
+        if (!any) break;
+        emu::launch(dim3(grid_x), dim3(kSweepThreads), true,
+                    [&] { batch_sweep_x_kernel<double, RefOrder, false, kSweepThreads, 1>(b, xt, 0); });
+        for (int stage = 1; stage <= 2; ++stage)
+            emu::launch(dim3(grid_y), dim3(kSweepThreads), false,
+                        [&] { batch_sweep_y_kernel<double, RefOrder, kSweepThreads, 1>(b, yt, stage); });
+        emu::launch(dim3(grid_x), dim3(kSweepThreads), true,
+                    [&] { batch_sweep_x_kernel<double, RefOrder, true, kSweepThreads, 1>(b, xt, 3); });
+        emu::launch(dim3(rb0[np]), dim3(kGhostThreads), true, [&] { batch_ghost_kernel<double, kGhostThreads>(b); });
+    }
+    c0 = 0;
+    for (int p = 0; p < np; ++p) {
+        for (int y = 0; y < ny[p]; ++y)
+            for (int x = 0; x < nx[p]; ++x)
+                for (int f = 0; f < 4; ++f)
+                    out_cells[c0 + 4 * ((long long)y * nx[p] + x) + f] =
+                        base[P[p].u + f * P[p].plane + (long long)y * P[p].pitch + x];
+        c0 += 4LL * nx[p] * ny[p];
+        out_t[p] = ctl[p].t;
+        out_steps[p] = ctl[p].steps;
+    }
     return 0;
 }
 

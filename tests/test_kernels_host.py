@@ -19,6 +19,11 @@ GPU:
   rows and the shock, only the problem's own edges filled);
 * the step size and end-of-loop decision of the reference's rule
   (src/wrappers.cuh:196-207, the oracle's orc_dt);
+* the batched kernels (2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh: problem
+  lookup, item chunks per warp across problem boundaries, per-problem step
+  control, tickets and wave-speed maxima, skipped items of finished
+  problems) solving six problems of mixed sizes and presets, each equal to
+  the oracle's solve of that problem alone;
 * the adjoint step's own kernels (2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc:
   the x and y sweep transposes, with the y tiles in shared memory and block
   barriers, and the ghost-ring transposes) as the transpose of the
@@ -54,6 +59,7 @@ def kh(tmp_path_factory):
     lib.kh_wave_speed.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
     lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     step = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int]
+    lib.kh_batch_solve.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3
     lib.kh_sweep32.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_step_jvp.argtypes = step + [ctypes.c_void_p] * 2
     lib.kh_step_vjp.argtypes = step + [ctypes.c_void_p]
@@ -277,3 +283,31 @@ def test_adjoint_kernels_transpose_the_forward_items(kh, oracle, pkg, strategy):
     assert np.abs(out - R).max() <= 1e-12 * np.abs(R).max()
     a, b = np.sum(Jv * w), np.sum(v * JTw)
     assert abs(a - b) <= 1e-13 * max(abs(a), abs(b)), (a, b)  # measured <= 1.6e-15
+
+
+@pytest.mark.parametrize("grid", [(1, 1), (3, 2)], ids=["one-block", "several-blocks"])
+def test_batched_kernels_equal_single_solves(kh, oracle, grid):
+    """Six problems of different sizes, presets and end times (the first one
+    ends after two steps, so its items are skipped afterwards) through the
+    batched kernels, 12 steps; each problem against the oracle alone."""
+    import ensemble_ranks
+
+    probs = ensemble_ranks.problems()[:6]
+    steps = 12
+    keys = ("width", "height", "t_end", "cfl", "alpha", "gamma", "strategy")
+    nx = np.array([U.shape[1] for U, _ in probs], dtype=np.int32)
+    ny = np.array([U.shape[0] for U, _ in probs], dtype=np.int32)
+    par = np.array([[kw[k] for k in keys] for _, kw in probs], dtype=np.float64)
+    cells = np.concatenate([np.ascontiguousarray(U[..., :4]).ravel() for U, _ in probs])
+    out, t, n = np.empty_like(cells), np.empty(len(probs)), np.empty(len(probs), dtype=np.int32)
+    assert kh.kh_batch_solve(len(probs), nx.ctypes.data, ny.ctypes.data, par.ctypes.data, cells.ctypes.data, 16,
+                             grid[0], grid[1], steps, out.ctypes.data, t.ctypes.data, n.ctypes.data) == 0
+    c = 0
+    for p, (U, kw) in enumerate(probs):
+        size = 4 * U.shape[0] * U.shape[1]
+        G = out[c:c + size].reshape(U.shape[0], U.shape[1], 4)
+        c += size
+        R, rsteps, rt = oracle.solve(U, max_steps=steps, **kw)
+        assert (int(n[p]), float(t[p])) == (rsteps, rt), p
+        assert np.array_equal(G, R, equal_nan=True), p
+    assert n[0] < steps  # one problem finished early and was skipped
