@@ -3,7 +3,8 @@
 // fvm2d_adjoint.inc, so that the CPU tests can compare it with the oracle
 // and with itself without a GPU: the ghost-ring rules (ghost_cell), the
 // step-size plan (plan_step), the wave speed, the sweep work items (x_item,
-// y_item) with the kernels' item numbering, the batched kernels
+// y_item) with the kernels' item numbering, whole solves through the
+// single-problem kernels, the batched kernels
 // (fvm2d_batch.cuh) over several problems, and the adjoint step's kernels
 // (adjoint_x_kernel, adjoint_y_kernel, the ghost transposes) against a
 // dual-number tangent of the forward items.  tests/test_kernels_host.py
@@ -644,6 +645,76 @@ int kh_batch_solve(int np, const int *nx, const int *ny, const double *params, c
         out_t[p] = ctl[p].t;
         out_steps[p] = ctl[p].steps;
     }
+    return 0;
+}
+
+// A solve through the single-problem kernels in the reference order
+// (RefOrder), launched as a solver's step graphs launch them: init_kernel,
+// then per step sweep_x_kernel, sweep_y_kernel twice, the final
+// sweep_x_kernel and ghost_kernel, on `blocks` blocks of 128 threads per
+// sweep (grid-stride), until the control record ends the loop or max_steps.
+// out: final state; t, steps and the health record's first bad step.
+int kh_solve(const double *cells, int nx, int ny, double width, double height, double t_end, double cfl,
+             double alpha, double gamma, int strategy, int T, int blocks, int max_steps, double *out, double *t,
+             int *steps, int *first_bad)
+{
+    constexpr int kNT = 128, kGhostNT = 256, kInitNT = 256;
+    if (nx < 6 || ny < 6 || blocks < 1) return 1;
+    const int pitch = (nx + 31) / 32 * 32;
+    const long long plane = (long long)pitch * ny;
+    std::vector<double> Uv(4 * plane, 0.0), Av(4 * plane, 0.0), Bv(4 * plane, 0.0);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            for (int f = 0; f < 4; ++f) Uv[f * plane + (long long)y * pitch + x] = cells[4 * ((long long)y * nx + x) + f];
+    const Field<double> U{Uv.data(), plane, pitch}, A{Av.data(), plane, pitch}, B{Bv.data(), plane, pitch};
+    StepControl ctl;
+    std::memset(&ctl, 0, sizeof ctl);
+    ctl.step_limit = max_steps;
+    const double hx = width / nx, hy = height / ny;
+    const PlanParams plan{t_end, cfl, hy < hx ? hy : hx, 0.0};
+    auto args = [&](const Field<double> &src, const Field<double> &dst, int dir) {
+        SweepArgs<double> a;
+        a.src = src;
+        a.dst = dst;
+        a.comb = dst;
+        a.flux = Field<double>{nullptr, plane, pitch};
+        a.nx = nx;
+        a.ny = ny;
+        a.h = dir == 0 ? hx : hy;
+        a.rh = 1.0 / a.h;
+        a.alpha = alpha;
+        a.gamma = gamma;
+        a.ctl = &ctl;
+        return a;
+    };
+    GhostArgs<double> g;
+    g.U = U;
+    g.nx = nx;
+    g.ny = ny;
+    g.strategy = strategy;
+    g.gamma = gamma;
+    g.ctl = &ctl;
+    g.plan = plan;
+    g.row0 = 0;
+    g.gny = ny;
+    g.fill_top = g.fill_bottom = 1;
+    const int ring = 4 * nx + 4 * (ny - 4);
+    emu::launch(dim3(2), dim3(kInitNT), true, [&] { init_kernel<double, kInitNT>(U, nx, ny, gamma, &ctl, plan); });
+    for (int k = 0; k < max_steps && ctl.active; ++k) {
+        const SweepArgs<double> ax = args(U, A, 0), ay = args(U, B, 1), aya = args(A, U, 1), axf = args(B, U, 0);
+        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<double, RefOrder, false, kNT, 1>(ax); });
+        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<double, RefOrder, kNT, 1>(ay, T); });
+        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<double, RefOrder, kNT, 1>(aya, T); });
+        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<double, RefOrder, true, kNT, 1>(axf); });
+        emu::launch(dim3((ring + kGhostNT - 1) / kGhostNT), dim3(kGhostNT), true,
+                    [&] { ghost_kernel<double, kGhostNT>(g); });
+    }
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            for (int f = 0; f < 4; ++f) out[4 * ((long long)y * nx + x) + f] = Uv[f * plane + (long long)y * pitch + x];
+    *t = ctl.t;
+    *steps = ctl.steps;
+    *first_bad = ctl.first_bad;
     return 0;
 }
 

@@ -19,6 +19,9 @@ GPU:
   rows and the shock, only the problem's own edges filled);
 * the step size and end-of-loop decision of the reference's rule
   (src/wrappers.cuh:196-207, the oracle's orc_dt);
+* whole solves through the single-problem kernels (sweep_x_kernel,
+  sweep_y_kernel, ghost_kernel with its last-block step commit, init_kernel)
+  on every preset, and their health record of the first bad step;
 * the batched kernels (2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh: problem
   lookup, item chunks per warp across problem boundaries, per-problem step
   control, tickets and wave-speed maxima, skipped items of finished
@@ -59,6 +62,8 @@ def kh(tmp_path_factory):
     lib.kh_wave_speed.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
     lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     step = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int]
+    lib.kh_solve.argtypes = ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 +
+                             [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4)
     lib.kh_batch_solve.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3
     lib.kh_sweep32.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_step_jvp.argtypes = step + [ctypes.c_void_p] * 2
@@ -311,3 +316,44 @@ def test_batched_kernels_equal_single_solves(kh, oracle, grid):
         assert (int(n[p]), float(t[p])) == (rsteps, rt), p
         assert np.array_equal(G, R, equal_nan=True), p
     assert n[0] < steps  # one problem finished early and was skipped
+
+
+def kernel_solve(kh, U, kw, blocks, max_steps, T=16):
+    U = np.ascontiguousarray(U[..., :4], dtype=np.float64)
+    ny, nx = U.shape[:2]
+    out = np.empty_like(U)
+    t, steps, bad = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    assert kh.kh_solve(U.ctypes.data, nx, ny, kw["width"], kw["height"], kw["t_end"], kw["cfl"], kw["alpha"],
+                       kw["gamma"], kw["strategy"], T, blocks, max_steps, out.ctypes.data, ctypes.byref(t),
+                       ctypes.byref(steps), ctypes.byref(bad)) == 0
+    return out, steps.value, t.value, bad.value
+
+
+@pytest.mark.parametrize("strategy", range(7))
+def test_single_problem_kernels_solve_like_the_oracle(kh, oracle, pkg, strategy):
+    """init_kernel, then the five kernels of a step as the step graphs launch
+    them, until the device control record ends the loop (the end time, for
+    the presets whose loops end before 15 steps) or 15 steps; one and three
+    blocks per sweep."""
+    nx, ny = 41, 30
+    U = pkg.scenarios.seeded_four_quadrant(nx, ny, 60 + strategy)
+    if strategy in (5, 6):
+        U = oracle.ghost(U, strategy)
+    kw = dict(width=1.0, height=0.7, t_end=0.02, cfl=0.45, alpha=ALPHA, gamma=GAMMA, strategy=strategy)
+    R, rsteps, rt = oracle.solve(U, max_steps=15, **kw)
+    for blocks in (1, 3):
+        V, steps, t, bad = kernel_solve(kh, U, kw, blocks, 15)
+        assert (steps, t, bad) == (rsteps, rt, 0), blocks
+        assert np.array_equal(V, R, equal_nan=True), blocks
+
+
+def test_health_record_names_the_first_bad_step(kh, pkg):
+    """A negative pressure planted in an interior cell is reported as step 1;
+    the run goes on, as the reference's does."""
+    nx, ny = 41, 30
+    U = np.ascontiguousarray(pkg.scenarios.seeded_four_quadrant(nx, ny, 3)[..., :4])
+    kw = dict(width=1.0, height=0.7, t_end=1.0, cfl=0.45, alpha=ALPHA, gamma=GAMMA, strategy=0)
+    assert kernel_solve(kh, U, kw, 2, 3)[3] == 0
+    U[12, 17, 1] = -1.0
+    V, steps, _, bad = kernel_solve(kh, U, kw, 2, 3)
+    assert bad == 1 and steps == 3
