@@ -370,9 +370,9 @@ def reference_arm(args, rank, world):
     }
 
 
+# ---------------------------------------------------------------------------
 # The other forms (batch, differentiation, vortex accuracy, FP32 precision),
 # each printed as its own JSON line.
-# The north star's other forms, each printed as its own JSON line.
 # ---------------------------------------------------------------------------
 def _batch_case(pkg, spec, precisions, label):
     sc = pkg.scenarios
