@@ -4,7 +4,7 @@
 // and with itself without a GPU: the ghost-ring rules (ghost_cell), the
 // step-size plan (plan_step), the wave speed, the sweep work items (x_item,
 // y_item) with the kernels' item numbering, whole solves through the
-// single-problem kernels, the batched kernels
+// single-problem kernels, the frame renderer and PNG writer, the batched kernels
 // (fvm2d_batch.cuh) over several problems, and the adjoint step's kernels
 // (adjoint_x_kernel, adjoint_y_kernel, the ghost transposes) against a
 // dual-number tangent of the forward items.  tests/test_kernels_host.py
@@ -200,6 +200,7 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint.inc"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_io.cuh"
 
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
@@ -716,6 +717,29 @@ int kh_solve(const double *cells, int nx, int ny, double width, double height, d
     *steps = ctl.steps;
     *first_bad = ctl.first_bad;
     return 0;
+}
+
+// A frame of a (ny, nx, 4) state as a solver writes one: the density range
+// reduced by density_range_blocks over `blocks` blocks of 256 threads, the
+// colours by render_density, the file by write_png_rgb.  Returns 0, or 2 when
+// the file cannot be written.
+int kh_frame(const double *cells, int nx, int ny, int blocks, const char *path)
+{
+    constexpr int kNT = 256;
+    if (nx < 1 || ny < 1 || blocks < 1) return 1;
+    const int pitch = (nx + 31) / 32 * 32;
+    std::vector<double> rho((size_t)pitch * ny, 0.0);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) rho[(size_t)y * pitch + x] = cells[4 * ((size_t)y * nx + x)];
+    std::vector<float> parts(2 * blocks);
+    std::vector<unsigned char> rgb(3 * (size_t)nx * ny);
+    emu::launch(dim3(blocks), dim3(kNT), true, [&] {
+        fvm2d::io::density_range_blocks<double, kNT>(rho.data(), pitch, nx, ny, parts.data());
+    });
+    emu::launch(dim3(3), dim3(kNT), false, [&] {
+        fvm2d::io::render_density<double>(rho.data(), pitch, nx, ny, parts.data(), blocks, rgb.data());
+    });
+    return fvm2d::io::write_png_rgb(path, nx, ny, rgb.data()) ? 0 : 2;
 }
 
 } // extern "C"

@@ -22,6 +22,9 @@ GPU:
 * whole solves through the single-problem kernels (sweep_x_kernel,
   sweep_y_kernel, ghost_kernel with its last-block step commit, init_kernel)
   on every preset, and their health record of the first bad step;
+* frames: the density range and viridis kernels and the PNG writer
+  (2d_fvm_cuda_b200/csrc/fvm2d_io.cuh) against a numpy rendering, the file
+  decoded with zlib (CRCs, Adler-32, stored blocks above 64 KiB);
 * the batched kernels (2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh: problem
   lookup, item chunks per warp across problem boundaries, per-problem step
   control, tickets and wave-speed maxima, skipped items of finished
@@ -64,6 +67,7 @@ def kh(tmp_path_factory):
     step = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int]
     lib.kh_solve.argtypes = ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 +
                              [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4)
+    lib.kh_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
     lib.kh_batch_solve.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3
     lib.kh_sweep32.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_step_jvp.argtypes = step + [ctypes.c_void_p] * 2
@@ -357,3 +361,30 @@ def test_health_record_names_the_first_bad_step(kh, pkg):
     U[12, 17, 1] = -1.0
     V, steps, _, bad = kernel_solve(kh, U, kw, 2, 3)
     assert bad == 1 and steps == 3
+
+
+@pytest.mark.parametrize("nx,ny,blocks", [(64, 48, 1), (200, 120, 4), (37, 5, 3)])
+def test_frames_match_a_numpy_rendering(kh, pkg, tmp_path, nx, ny, blocks):
+    from test_frames_gpu import read_png, render
+
+    U = np.ascontiguousarray(pkg.scenarios.seeded_four_quadrant(nx, ny, 8)[..., :4])
+    U[..., 0] *= 1.0 + 0.01 * np.sin(np.arange(nx))[None, :]  # more than four density values
+    path = str(tmp_path / "f.png")
+    assert kh.kh_frame(U.ctypes.data, nx, ny, blocks, path.encode()) == 0
+    img = read_png(path)  # checks the chunk CRCs and, through zlib, the Adler-32
+    want = render(U[..., 0])
+    d = np.abs(img.astype(int) - want.astype(int))
+    assert img.shape == (ny, nx, 3)
+    assert d.max() <= 3 and (d == 0).mean() > 0.99  # a level can differ at a rounding tie
+    if 3 * nx * ny + ny > 65535:  # several stored blocks
+        assert os.path.getsize(path) > 65535
+
+
+def test_frame_of_a_uniform_density(kh, tmp_path):
+    U = np.ones((20, 30, 4))
+    path = str(tmp_path / "u.png")
+    assert kh.kh_frame(U.ctypes.data, 30, 20, 2, path.encode()) == 0
+    from test_frames_gpu import read_png
+
+    img = read_png(path)
+    assert np.all(img == img[0, 0]) and tuple(img[0, 0]) == (68, 1, 84)  # level 0: the first viridis stop
