@@ -10,188 +10,9 @@
 // dual-number tangent of the forward items.  tests/test_kernels_host.py
 // builds it and calls it through ctypes.
 //
-// Launches are emulated block by block.  Kernels with warp shuffles or block
-// barriers run one host thread per CUDA thread: a shuffle is an exchange
-// through per-lane slots between two barriers of the warp's 32 threads (a
-// butterfly shuffle and a vote likewise), __syncthreads a barrier of the
-// block's threads, atomics take a lock, and __shared__ arrays are
-// static (one block runs at a time).  Kernels with neither run their threads
-// one after another.  The block-level reductions and atomics of the forward
-// kernels themselves are declared so that the headers compile; nothing called
-// here reaches them.
-#include <atomic>
-#include <cmath>
-#include <cstring>
-#include <mutex>
-#include <thread>
-#include <type_traits>
-#include <vector>
-
-#include <cuda_runtime.h>
-
-#undef __shared__
-#define __shared__ static
-
-static thread_local uint3 threadIdx;
-static uint3 blockIdx;
-static dim3 blockDim, gridDim;
-
-namespace emu {
-constexpr int kLanes = 32, kMaxWarps = 32;
-
-// Generation barrier of n threads; waiters yield rather than sleep (the
-// emulated warps run far more threads than cores, and a barrier releases
-// within microseconds).
-struct Barrier {
-    std::atomic<int> count{0}, gen{0};
-    int n = kLanes;
-    void wait()
-    {
-        const int g = gen.load(std::memory_order_acquire);
-        if (count.fetch_add(1, std::memory_order_acq_rel) == n - 1) {
-            count.store(0, std::memory_order_relaxed);
-            gen.fetch_add(1, std::memory_order_release);
-        } else {
-            while (gen.load(std::memory_order_acquire) == g) std::this_thread::yield();
-        }
-    }
-};
-static Barrier warp_bar[kMaxWarps];
-static Barrier block_bar;
-static unsigned char slot[kMaxWarps][kLanes][16];
-
-inline int flat_thread() { return int(threadIdx.x + threadIdx.y * blockDim.x); }
-
-// value of lane (lane + delta) of the caller's warp, or the caller's own
-// where that lane is outside the warp, as the hardware shuffles do
-template <typename T>
-T exchange(T v, int delta)
-{
-    static_assert(sizeof(T) <= sizeof(slot[0][0]), "shuffle operand too wide");
-    const int f = flat_thread(), w = f / kLanes, lane = f % kLanes;
-    std::memcpy(slot[w][lane], &v, sizeof(T));
-    warp_bar[w].wait();
-    T r = v;
-    const int src = lane + delta;
-    if (src >= 0 && src < kLanes) std::memcpy(&r, slot[w][src], sizeof(T));
-    warp_bar[w].wait();
-    return r;
-}
-
-// lane ^ mask's value (butterfly shuffle)
-template <typename T>
-T exchange_xor(T v, int mask)
-{
-    const int lane = flat_thread() % kLanes;
-    return exchange(v, (lane ^ mask) - lane);
-}
-
-// warp vote: nonzero if any lane's predicate is
-inline int vote_any(int pred)
-{
-    const int f = flat_thread(), w = f / kLanes, lane = f % kLanes;
-    std::memcpy(slot[w][lane], &pred, sizeof pred);
-    warp_bar[w].wait();
-    int any = 0;
-    for (int l = 0; l < kLanes; ++l) {
-        int q;
-        std::memcpy(&q, slot[w][l], sizeof q);
-        any |= q != 0;
-    }
-    warp_bar[w].wait();
-    return any;
-}
-
-static std::mutex atomic_mutex;  // the atomics of threaded launches
-
-// Runs `body` as the kernel body of every thread of every block of the grid:
-// `threaded` for kernels that shuffle or wait at block barriers (whole warps
-// of threads), else thread after thread.
-template <class F>
-void launch(dim3 grid, dim3 block, bool threaded, F body)
-{
-    gridDim = grid;
-    blockDim = block;
-    const int nt = int(block.x * block.y);
-    block_bar.n = nt;
-    for (unsigned by = 0; by < grid.y; ++by)
-        for (unsigned bx = 0; bx < grid.x; ++bx) {
-            blockIdx = make_uint3(bx, by, 0);
-            auto run = [&](int t) {
-                threadIdx = make_uint3(unsigned(t) % block.x, unsigned(t) / block.x, 0);
-                body();
-            };
-            if (threaded) {
-                std::vector<std::thread> th;
-                for (int t = 0; t < nt; ++t) th.emplace_back(run, t);
-                for (auto &x : th) x.join();
-            } else {
-                for (int t = 0; t < nt; ++t) run(t);
-            }
-        }
-}
-} // namespace emu
-
-static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
-static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
-// sm_100's two-wide FP32 instructions: two correctly rounded operations
-static inline float2 __fadd2_rn(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-static inline float2 __fmul2_rn(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
-static inline float2 __ffma2_rn(float2 a, float2 b, float2 c)
-{
-    return make_float2(std::fma(a.x, b.x, c.x), std::fma(a.y, b.y, c.y));
-}
-template <typename T>
-static inline T __shfl_xor_sync(unsigned, T v, int m) { return emu::exchange_xor(v, m); }
-template <typename T>
-static inline T __shfl_down_sync(unsigned, T v, int d) { return emu::exchange(v, d); }
-template <typename T>
-static inline T __shfl_up_sync(unsigned, T v, int d) { return emu::exchange(v, -d); }
-template <typename T>
-static inline T __shfl_sync(unsigned, T v, int) { return v; }
-static inline void __syncthreads() { emu::block_bar.wait(); }
-static inline void __threadfence() {}
-static inline int __any_sync(unsigned, int p) { return emu::vote_any(p); }
-static inline long long __double_as_longlong(double x)
-{
-    long long r;
-    std::memcpy(&r, &x, 8);
-    return r;
-}
-static inline double __longlong_as_double(long long x)
-{
-    double r;
-    std::memcpy(&r, &x, 8);
-    return r;
-}
-template <typename T>
-static inline T atomicAdd(T *p, T v)
-{
-    std::lock_guard<std::mutex> g(emu::atomic_mutex);
-    const T o = *p;
-    *p = o + v;
-    return o;
-}
-template <typename T>
-static inline T atomicMax(T *p, T v)
-{
-    std::lock_guard<std::mutex> g(emu::atomic_mutex);
-    const T o = *p;
-    if (v > o) *p = v;
-    return o;
-}
-template <typename T>
-static inline T atomicCAS(T *p, T c, T v)
-{
-    std::lock_guard<std::mutex> g(emu::atomic_mutex);
-    const T o = *p;
-    if (o == c) *p = v;
-    return o;
-}
-#pragma GCC diagnostic ignored "-Wunknown-pragmas"
-static inline int min(int a, int b) { return a < b ? a : b; }
-static inline int max(int a, int b) { return a > b ? a : b; }
-#define __launch_bounds__(...)
+// The CUDA built-ins are emulated on the host by cuda_host_emu.h; the sweeps,
+// steps and transposes are composed in kernels_host_steps.h.
+#include "cuda_host_emu.h"
 
 #define FVM2D_VARIANT host
 #define FVM2D_REAL double
@@ -205,141 +26,8 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
 
-namespace {
+#include "kernels_host_steps.h"
 
-// Four planes of pitch nx for a (ny, nx) array.
-template <typename R>
-struct Planes {
-    int nx = 0, ny = 0;
-    long long plane = 0;
-    std::vector<R> v;
-    Planes() = default;
-    Planes(int nx_, int ny_) : nx(nx_), ny(ny_), plane((long long)nx_ * ny_), v(4 * plane, R(0.0)) {}
-    Field<R> field() { return Field<R>{v.data(), plane, nx}; }
-};
-
-template <typename R>
-SweepArgs<R> sweep_args(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double alpha, double gamma)
-{
-    SweepArgs<R> a;
-    a.src = src.field();
-    a.dst = dst.field();
-    a.comb = a.dst;
-    a.flux = flux ? flux->field() : Field<R>{nullptr, src.plane, src.nx};
-    a.nx = src.nx;
-    a.ny = src.ny;
-    a.h = h;
-    a.rh = 1.0 / h;
-    a.alpha = alpha;
-    a.gamma = gamma;
-    a.ctl = nullptr;
-    return a;
-}
-
-// x-sweep src -> dst through x_item on one emulated warp (FINAL: dst holds
-// branch A and is averaged in place); TAPE stores the interface fluxes.
-template <typename R, bool FINAL, bool TAPE, class Phys = Hoisted>
-void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma)
-{
-    const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
-    const SweepConsts<R> K = sweep_consts(a, dt);
-    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
-    const long long nwork = (long long)nseg * a.ny;
-    emu::launch(dim3(1), dim3(32), true, [&] {
-        double vmax = 0.0;
-        int bad = 0;
-        for (long long w = 0; w < nwork; ++w)
-            x_item<R, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
-    });
-}
-
-// y-sweep src -> dst through y_item, segments of T interfaces.
-template <typename R, bool TAPE, class Phys = Hoisted>
-void y_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double dt, double alpha, double gamma, int T)
-{
-    const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
-    const SweepConsts<R> K = sweep_consts(a, dt);
-    const int ncw = (a.nx + 31) / 32, nseg = y_segments(a.ny, T);
-    for (int seg = 0; seg < nseg; ++seg)
-        for (int cw = 0; cw < ncw; ++cw)
-            for (int lane = 0; lane < 32; ++lane) y_item<R, Phys, TAPE>(a, K, seg, nseg, cw, lane, T);
-}
-
-// One split step U -> out of the shared-reciprocal build, in the kernels'
-// order (X(U) -> A, Y(U) -> B, Y(A) -> out, X(B) averaged with out, ghost
-// fill of out at t + dt); TAPE keeps A, B and the four sweeps' fluxes.
-template <typename R, bool TAPE>
-void forward_step(Planes<R> &U, Planes<R> &A, Planes<R> &B, Planes<R> &out, Planes<R> *flux, int strategy, double t,
-                  double dt, double hx, double hy, double alpha, double gamma, int T)
-{
-    x_sweep<R, false, TAPE>(U, A, TAPE ? &flux[0] : nullptr, hx, dt, alpha, gamma);
-    y_sweep<R, TAPE>(U, B, TAPE ? &flux[1] : nullptr, hy, dt, alpha, gamma, T);
-    y_sweep<R, TAPE>(A, out, TAPE ? &flux[2] : nullptr, hy, dt, alpha, gamma, T);
-    x_sweep<R, true, TAPE>(B, out, TAPE ? &flux[3] : nullptr, hx, dt, alpha, gamma);
-    GhostArgs<R> g;
-    g.U = out.field();
-    g.nx = U.nx;
-    g.ny = U.ny;
-    g.strategy = strategy;
-    g.gamma = gamma;
-    g.ctl = nullptr;
-    g.plan = fvm2d::PlanParams{};
-    g.row0 = 0;
-    g.gny = U.ny;
-    g.fill_top = g.fill_bottom = 1;
-    for (int k = 0; k < 4 * U.nx + 4 * (U.ny - 4); ++k) ghost_cell(g, k, t + dt);
-}
-
-template <typename R>
-void cells_to(Planes<R> &P, const double *cells, const double *tangent)
-{
-    for (long long c = 0; c < P.plane; ++c)
-        for (int f = 0; f < 4; ++f) {
-            if constexpr (std::is_same_v<R, Dual>)
-                P.v[f * P.plane + c] = R(cells[4 * c + f], tangent[4 * c + f]);
-            else
-                P.v[f * P.plane + c] = R(cells[4 * c + f]);
-        }
-}
-
-// The sweep transposes' constants, formed as the adjoint step's launcher
-// forms them (the forward's sweep_consts: lambda = dt / h).
-SweepConsts<A> adjoint_consts(double h, double dt, double alpha, double gamma)
-{
-    SweepConsts<A> K;
-    K.h = h;
-    K.rh = 1.0 / h;
-    K.alpha = alpha;
-    K.g = gamma;
-    K.k = dt;
-    K.lambda = dt / h;
-    K.igm1 = 1.0 / (gamma - 1.0);
-    K.kappa = (gamma + 1.0) / 2.0;
-    return K;
-}
-
-// out = (d sweep_dir at U)^T ub (+ addend), with the grids the launcher uses
-// (adjoint_x_kernel grid-strides, here one block of 128 threads).
-void transpose(int dir, Planes<double> &U, Planes<double> &F, Planes<double> &ub, Planes<double> &out,
-               Planes<double> *addend, double h, double dt, double alpha, double gamma)
-{
-    SweepT g;
-    g.U = U.field();
-    g.F = F.field();
-    g.ub = ub.field();
-    g.out = out.field();
-    g.addend = addend ? addend->field() : Field<double>{nullptr, U.plane, U.nx};
-    g.nx = U.nx;
-    g.ny = U.ny;
-    g.K = adjoint_consts(h, dt, alpha, gamma);
-    if (dir == 0)
-        emu::launch(dim3(1), dim3(ANT), true, [&] { adjoint_x_kernel(g); });
-    else
-        emu::launch(dim3((U.nx + kTileCols - 1) / kTileCols, (U.ny + kLineOut - 1) / kLineOut), dim3(ANT), true,
-                    [&] { adjoint_y_kernel(g); });
-}
-
-} // namespace
 using fvm2d::PlanParams;
 using fvm2d::StepControl;
 
