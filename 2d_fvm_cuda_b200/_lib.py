@@ -57,6 +57,7 @@ SIGNATURES = [
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
     ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_measure_fp64_peak", ctypes.c_int, [_dp, _dp]),
     ("fvm2d_set_fixed_dt", ctypes.c_int, [_vp, ctypes.c_double]),
     ("fvm2d_jvp", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
     ("fvm2d_forward", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
@@ -112,6 +113,14 @@ def load() -> ctypes.CDLL:
 def check(rc: int) -> None:
     if rc != FVM2D_OK:
         raise FVM2DError(rc, load().fvm2d_last_error().decode())
+
+
+def measure_fp64_peak() -> tuple[float, float]:
+    """(TFLOP/s, ms per launch) of fvm2d_measure_fp64_peak on the current device."""
+    lib = load()
+    tf, ms = ctypes.c_double(0), ctypes.c_double(0)
+    check(lib.fvm2d_measure_fp64_peak(ctypes.byref(tf), ctypes.byref(ms)))
+    return tf.value, ms.value
 
 
 def as_cells(U) -> np.ndarray:

@@ -18,6 +18,10 @@
 // caller.  The array keeps whatever the previous call left; the control
 // record, the only part that must start from known values, is rewritten at
 // the start of every call.
+//
+// A call waits for its own work (it reads the step-control record back
+// between groups of steps), so it cannot be made while its stream is being
+// captured into a CUDA graph; such a call is refused.
 #include "../../include/fvm2d.h"
 #include "fvm2d_control.h"
 
@@ -38,6 +42,10 @@ static __device__ __align__(256) double g_scratch[kScratchDoubles + kControlDoub
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double *g_scratch_ptr[kMaxDevices] = {};  // device address of g_scratch, per device
+
+// Steps enqueued between two reads of the control record: a run that reaches
+// its end time early stops within this many (empty) steps of it.
+constexpr int kStepsPerCheck = 32;
 
 int fail(int code, const std::string &msg) { return fvm2d::report_error(code, msg.c_str()); }
 
@@ -112,7 +120,20 @@ int fvm2d_advance_noalloc(const double *state_in, double *state_out, int nx, int
     if (int rc = setup_device(dev, &scratch)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(s, &capturing))) return cuda_fail(e, "cudaStreamIsCapturing");
+    if (capturing != cudaStreamCaptureStatusNone)
+        return fail(FVM2D_ERR_INVALID, "fvm2d_advance_noalloc waits for its work and cannot run inside a stream capture");
+
     const long long plane = (long long)nx * ny;
+    {
+        // the same buffer, or two that do not overlap: a partial overlap would
+        // make the input copy below read cells it has already overwritten
+        const char *in0 = reinterpret_cast<const char *>(state_in), *out0 = reinterpret_cast<const char *>(state_out);
+        const long long bytes = (long long)sizeof(double) * 4 * plane;
+        if (in0 != out0 && in0 < out0 + bytes && out0 < in0 + bytes)
+            return fail(FVM2D_ERR_INVALID, "state_in and state_out overlap without being the same buffer");
+    }
     if (state_out != state_in &&
         (e = cudaMemcpyAsync(state_out, state_in, sizeof(double) * 4 * plane, cudaMemcpyDeviceToDevice, s)))
         return cuda_fail(e, "copy of the input state");
@@ -141,12 +162,19 @@ int fvm2d_advance_noalloc(const double *state_in, double *state_out, int nx, int
     reset_control<<<1, 32, 0, s>>>(c.ctl, t0, nsteps);
     if ((e = cudaGetLastError())) return cuda_fail(e, "control reset");
     if ((e = fvm2d::fp64::enqueue_init(c, s))) return cuda_fail(e, "init kernel");
-    for (int k = 0; k < nsteps; ++k)
-        if ((e = fvm2d::fp64::enqueue_step(c, s, nullptr))) return cuda_fail(e, "step kernels");
-
+    // groups of steps, each followed by a read of the control record: once the
+    // run has reached t_end (or nsteps) no further steps are enqueued
     fvm2d::StepControl out;
-    if ((e = cudaMemcpyAsync(&out, c.ctl, sizeof(out), cudaMemcpyDeviceToHost, s))) return cuda_fail(e, "control read");
-    if ((e = cudaStreamSynchronize(s))) return cuda_fail(e, "cudaStreamSynchronize");
+    int queued = 0;
+    do {
+        const int n = (nsteps - queued < kStepsPerCheck) ? nsteps - queued : kStepsPerCheck;
+        for (int k = 0; k < n; ++k)
+            if ((e = fvm2d::fp64::enqueue_step(c, s, nullptr))) return cuda_fail(e, "step kernels");
+        queued += n;
+        if ((e = cudaMemcpyAsync(&out, c.ctl, sizeof(out), cudaMemcpyDeviceToHost, s)))
+            return cuda_fail(e, "control read");
+        if ((e = cudaStreamSynchronize(s))) return cuda_fail(e, "cudaStreamSynchronize");
+    } while (out.active && queued < nsteps);
     if (t_out) *t_out = out.t;
     if (steps_out) *steps_out = out.steps;
     return FVM2D_OK;

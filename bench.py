@@ -292,6 +292,16 @@ def product_arm(args, rank, world, local_rank):
             adjoint = adjoint_summary(pkg)
         except Exception as e:  # noqa: BLE001
             adjoint = {"error": f"{type(e).__name__}: {e}"}
+        # the FP32 form's error on the two long runs it is specified on
+        # (configs 1 and 2), one GPU only: a few minutes of device time
+        fp32_configs = None
+        if world == 1 and not args.no_configs:
+            fp32_configs = {}
+            for key, fn in (("vortex_2000", form_vortex), ("shock_bubble_4096", form_precision)):
+                try:
+                    fp32_configs[key] = fn(args, with_reference_order=False)
+                except Exception as e:  # noqa: BLE001
+                    fp32_configs[key] = {"error": f"{type(e).__name__}: {e}"}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
@@ -314,9 +324,13 @@ def product_arm(args, rank, world, local_rank):
                          "kernel_ms": dict(zip(["sweep_x", "sweep_y_1", "sweep_y_2", "sweep_x_final", "ghost_fill"],
                                                kernel_ms))},
             "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} four-quadrant, {csteps} steps in {cs:.1f} s"},
+                             "sample": f"{CPU_SAMPLE_N}x{CPU_SAMPLE_N} four-quadrant, {csteps} steps in {cs:.1f} s",
+                             "sample_note": "a 1024^2 sample of the 4096^2 workload: its 34 MB of state sit in "
+                                            "the host caches more than 4096^2 would, so the CPU rate is if "
+                                            "anything favourable to the CPU"},
             "reference_cuda": ref_cuda,
             "fp32": fp32,
+            "fp32_configs": fp32_configs,
             "adjoint": adjoint,
             "clocks": clocks,
             "gpu_launches": launches,
@@ -577,10 +591,12 @@ def form_adjoint(args):
             "wall_s": {"forward": t1 - t0, "vjp": t2 - t1}}
 
 
-def form_vortex(args):
+def form_vortex(args, with_reference_order=False):
     """Isentropic vortex of strength 5 on periodic [0,10]^2, 2000^2 array,
     background (1,1,1,1), advected one period (t_end 10), CFL 0.45: FP64 and
-    FP32 error against the exact (translated) vortex and FP32 against FP64."""
+    FP32 error against the exact (translated) vortex and FP32 against FP64.
+    (Periodic is one of the presets the reference lacks: its parity rests on
+    the oracle's restatement of the preset.)"""
     pkg = importlib.import_module("2d_fvm_cuda_b200")
     sc = pkg.scenarios
     n = 2000
@@ -609,22 +625,29 @@ def form_vortex(args):
     res["fp32"]["rho_rel_l1_vs_fp64"] = rl1(states["fp32"], states["fp64"])
     res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(states["fp32"][inner][..., 0] - states["fp64"][inner][..., 0]).max())
     res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
+    res["fp32"]["rho_rel_l1_target"] = 1e-5
     return {"form": "vortex", "workload": "2000^2 periodic isentropic vortex, one period", "results": res}
 
 
-def form_precision(args):
+def form_precision(args, with_reference_order=True):
     """Precision form: 4096^2 Mach-2 shock hitting a light bubble (rho 0.1,
     radius 0.15, 8 seeded boundary modes of total amplitude <= 0.01) in a
     [0,2]x[0,1] channel, reflective top/bottom, transmissive left/right,
     t_end 0.4, CFL 0.45: the FP32 build (compensated update, FP64 dt) against
-    the FP64 build, density L1 and Linf, and their speeds."""
+    the FP64 build, density L1 and Linf, and their speeds.  (Reflective
+    top/bottom walls are a preset the reference lacks: parity rests on the
+    oracle's restatement of it.)"""
     pkg = importlib.import_module("2d_fvm_cuda_b200")
     n = args.n
     U0 = pkg.scenarios.shock_bubble(n, n, width=2.0, height=1.0, seed=0)
     res, states = {}, {}
     # FP64_REFORDER (the reference's operation order) differs from FP64 by
-    # rounding only: how far two FP64 runs drift apart on this flow
-    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32"), (pkg.FP64_REFORDER, "fp64_reference_order")):
+    # rounding only: how far two FP64 runs drift apart on this flow (five
+    # times slower than FP64, so left out of the default bench line)
+    builds = [(pkg.FP64, "fp64"), (pkg.FP32, "fp32")]
+    if with_reference_order:
+        builds.append((pkg.FP64_REFORDER, "fp64_reference_order"))
+    for prec, name in builds:
         h = pkg.Handle(n, n)
         h.configure(2.0, 1.0, 0.4, 0.45, 1.9, 1.4, 6, prec)
         h.set_state(U0)
@@ -638,9 +661,11 @@ def form_precision(args):
     res["fp32"]["rho_rel_l1_vs_fp64"] = float(np.abs(S - D).sum() / np.abs(D).sum())
     res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(S - D).max())
     res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
-    Rf = states["fp64_reference_order"]
-    res["fp64_reference_order"]["rho_rel_l1_vs_fp64"] = float(np.abs(Rf - D).sum() / np.abs(D).sum())
-    res["fp64_reference_order"]["rho_linf_vs_fp64"] = float(np.abs(Rf - D).max())
+    res["fp32"]["rho_rel_l1_target"] = 1e-5
+    if with_reference_order:
+        Rf = states["fp64_reference_order"]
+        res["fp64_reference_order"]["rho_rel_l1_vs_fp64"] = float(np.abs(Rf - D).sum() / np.abs(D).sum())
+        res["fp64_reference_order"]["rho_linf_vs_fp64"] = float(np.abs(Rf - D).max())
     return {"form": "precision", "workload": f"{n}^2 Mach-2 shock-bubble, [0,2]x[0,1], t_end 0.4", "results": res}
 
 
@@ -655,6 +680,8 @@ def main():
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="arithmetic of a --kernels-only run")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="leave the FP32 config-1/config-2 error runs out of the default line")
     ap.add_argument("--form", choices=["batch", "adjoint", "vortex", "precision"],
                     help="measure one of the other forms instead (one JSON line, rank 0, one GPU)")
     args = ap.parse_args()

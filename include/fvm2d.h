@@ -225,6 +225,13 @@ int fvm2d_get_run_stats(fvm2d_solver *s, double *device_ms, long long *kernel_la
  * fvm2d_advance.  No reference counterpart (diagnostics). */
 int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *steps_done);
 
+/* The current device's FP64 rate in TFLOP/s (2 flops per fused multiply-add):
+ * a fully occupied grid of independent FMA chains, best of ten CUDA-event
+ * timed launches (*ms_per_launch, may be NULL, receives that launch's time).
+ * The FP64-pipe roofline of the sweeps is quoted against it.  No reference
+ * counterpart (diagnostics). */
+int fvm2d_measure_fp64_peak(double *tflops, double *ms_per_launch);
+
 /* ---- differentiation (no reference counterpart) ----------------------------
  * Derivatives of the step with respect to the state, at a fixed step size so
  * the CFL maximum is not differentiated: fvm2d_forward / fvm2d_vjp on the
@@ -325,17 +332,23 @@ int fvm2d_batch_autotune(fvm2d_batch *b, int trial_steps, int *segment_interface
  *
  * state_in, state_out: device memory, 4 planes (rho, p, u, v) of ny x nx
  *   doubles each, row-major, planes back to back; they may be the same
- *   buffer.  The result (and the whole ring of ghost cells) lands in
- *   state_out.
+ *   buffer, but two buffers that overlap only in part are rejected with
+ *   FVM2D_ERR_INVALID.  The result (and the whole ring of ghost cells) lands
+ *   in state_out.
  * Parameters as the solver setters (fvm2d_set_spatial_layout, ...), t_end
  *   bounding the run as the reference's end time does; *t_out and
  *   *steps_out (may be NULL) receive the time reached and the steps taken.
  * stream: a cudaStream_t (NULL for the default stream); the call returns
- *   after the work on it has finished.
+ *   after the work on it has finished.  Steps are enqueued in groups of 32
+ *   with a read of the step-control record after each group, so a run that
+ *   reaches t_end early stops within 32 steps of it: nsteps may be a generous
+ *   upper bound.
+ * The call waits for its own work, so it cannot run inside a stream capture:
+ *   a call on a stream that is being captured is rejected with
+ *   FVM2D_ERR_INVALID.
  * The first call on each device finds the device address of the static
- * array and sets kernel attributes; make that first call before any stream
- * capture.  All calls share the array: calls whose GPU work overlaps race on
- * it, so serialize them. */
+ * array and sets kernel attributes.  All calls share the array: calls whose
+ * GPU work overlaps race on it, so serialize them. */
 int fvm2d_advance_noalloc(const double *state_in, double *state_out, int nx, int ny, double width, double height,
                           double t_end, double cfl, double alpha, double gamma, int strategy, double t0,
                           int nsteps, void *stream, double *t_out, int *steps_out);

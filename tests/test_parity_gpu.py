@@ -109,6 +109,34 @@ def test_fma_within_tolerance_full_quadrant_workload(pkg, oracle, golden, precis
     assert (ssteps, st) == (osteps, ot) and np.array_equal(S, O)
 
 
+def test_fma_within_tolerance_after_every_step_of_the_quadrant_workload(pkg, oracle, golden):
+    """The 400x400 workload compared step by step: after each of its 620
+    steps the product build (FP64, shared reciprocals, FMA) stays within the
+    relative L1 tolerance of the oracle in every field, and its step size
+    within a few ulp of the oracle's."""
+    z, manifest = golden
+    m = manifest["quad_outflow_400x400_seed0"]
+    kw = {k: m[k] for k in RUN_KEYS}
+    U = pkg.scenarios.seeded_four_quadrant(m["nx"], m["ny"], m["seed"])
+    h = pkg.Handle(m["nx"], m["ny"])
+    h.configure(kw["width"], kw["height"], kw["t_end"], kw["cfl"], kw["alpha"], kw["gamma"], kw["strategy"], pkg.FP64)
+    h.set_state(U)
+    t, worst = 0.0, 0.0
+    for k in range(m["steps"]):
+        r = oracle.step(U, t=t, **kw)
+        assert r is not None, f"the oracle's loop ended after {k} steps"
+        U, t, dt = r
+        assert h.advance(1) == 1, f"the product's loop ended after {k} steps"
+        tg, sg, dtg = h.time()
+        assert sg == k + 1 and dtg == pytest.approx(dt, rel=1e-14, abs=0)
+        err = max(rel_l1(h.get_state(4), U))
+        assert err <= REL_L1_TOL, f"step {k + 1}: relative L1 {err}"
+        worst = max(worst, err)
+    assert h.advance(1) == 0 and oracle.step(U, t=t, **kw) is None  # both loops end after the same step
+    h.close()
+    print(f"620 steps, largest relative L1 after any step: {worst:.3g}")
+
+
 @pytest.mark.skipif(not os.path.exists(REF_GPU_NOFMA), reason="reference CUDA build not present")
 def test_reference_cuda_nofma_equals_strict(pkg):
     U0 = pkg.scenarios.seeded_four_quadrant(96, 64, 77)
