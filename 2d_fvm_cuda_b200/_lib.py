@@ -52,12 +52,19 @@ SIGNATURES = [
     ("fvm2d_set_row_frame", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("fvm2d_get_rows", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
     ("fvm2d_set_rows", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    ("fvm2d_get_stream", ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    ("fvm2d_get_rows_async", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    ("fvm2d_set_rows_async", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    ("fvm2d_slab_begin", ctypes.c_int, [_vp, _vp]),
+    ("fvm2d_slab_step", ctypes.c_int, [_vp, _vp, _vp]),
+    ("fvm2d_slab_sync", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_get_computation_time_ms", ctypes.c_int, [_vp, _dp]),
     ("fvm2d_get_time_stages_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_get_time", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int), _dp]),
     ("fvm2d_get_run_stats", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     ("fvm2d_profile_kernels", ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_measure_fp64_peak", ctypes.c_int, [_dp, _dp]),
+    ("fvm2d_eval_reciprocals", ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp]),
     ("fvm2d_set_fixed_dt", ctypes.c_int, [_vp, ctypes.c_double]),
     ("fvm2d_jvp", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
     ("fvm2d_forward", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
@@ -290,6 +297,31 @@ class Handle:
 
     def set_rows_ptr(self, j0: int, nrows: int, ptr: int) -> None:
         check(self.lib.fvm2d_set_rows(self.h, int(j0), int(nrows), ptr))
+
+    # asynchronous slab steps: enqueued on the handle's stream, no host wait
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t (for torch.cuda.ExternalStream)."""
+        p = ctypes.c_void_p(0)
+        check(self.lib.fvm2d_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def get_rows_async(self, j0: int, nrows: int, ptr: int) -> None:
+        check(self.lib.fvm2d_get_rows_async(self.h, int(j0), int(nrows), ptr))
+
+    def set_rows_async(self, j0: int, nrows: int, ptr: int) -> None:
+        check(self.lib.fvm2d_set_rows_async(self.h, int(j0), int(nrows), ptr))
+
+    def slab_begin(self, smax_out_ptr: int) -> None:
+        check(self.lib.fvm2d_slab_begin(self.h, smax_out_ptr))
+
+    def slab_step(self, smax_in_ptr: int, smax_out_ptr: int) -> None:
+        check(self.lib.fvm2d_slab_step(self.h, smax_in_ptr, smax_out_ptr))
+
+    def slab_sync(self):
+        """(t, steps, done) after the enqueued slab steps have run."""
+        t, k, d = ctypes.c_double(0), ctypes.c_int(0), ctypes.c_int(0)
+        check(self.lib.fvm2d_slab_sync(self.h, ctypes.byref(t), ctypes.byref(k), ctypes.byref(d)))
+        return t.value, k.value, bool(d.value)
 
     # -- differentiation (fixed dt; forward/vjp on FP64 or FP32, jvp on FP64) --
     def set_fixed_dt(self, dt: float) -> None:

@@ -63,7 +63,7 @@ __device__ __forceinline__ Cell<A> update_adjoint(const Cell<A> &U, const Cell<A
     const A n0 = U.rho - (FR.rho - FL.rho) * K.lambda;
     const A n1 = m1 - (FR.p - FL.p) * K.lambda;
     const A n3 = m3 - (FR.ut - FL.ut) * K.lambda;
-    const A ir = A(1) / n0;
+    const A ir = rrcp(n0);
     // reverse of the primitive recovery
     A n0b = Ub.rho, n1b = ir * Ub.un, n3b = ir * Ub.ut, n2b = gm1 * Ub.p;
     A irb = n1 * Ub.un + n3 * Ub.ut;
@@ -106,7 +106,7 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
     // (the reverse below uses only what they are: irl = 1/rho_l,
     // il = 1/(rho_l a_l), a_l = sqrt(g pi_l / rho_l), icl = 1/c_l,
     // isum = 1/(c_l + c_r), and the same on the right) ----
-    const A irlr = one / (rho_l * rho_r);
+    const A irlr = rrcp(rho_l * rho_r);
     const A irl = rho_r * irlr, irr = rho_l * irlr;
     const A e_l = pi_l * irl * igm1, e_r = pi_r * irr * igm1;
     const A X_l = pi_lx - pi_l * rho_lx * irl, X_r = pi_rx - pi_r * rho_rx * irr;
@@ -121,19 +121,19 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
     if (right_first) {
         zl_arg = (pi_r - pi_l) * ir + du;
         c_l = rho_l * (a_l + kappa * rmax(zero, zl_arg));
-        icl = one / c_l;
+        icl = rrcp(c_l);
         zr_arg = (pi_l - pi_r) * icl + du;
         c_r = rho_r * (a_r + kappa * rmax(zero, zr_arg));
-        const A sc = c_l + c_r, q = one / (c_r * sc);
+        const A sc = c_l + c_r, q = rrcp(c_r * sc);
         icr = sc * q;
         isum = c_r * q;
     } else {
         zr_arg = (pi_l - pi_r) * il + du;
         c_r = rho_r * (a_r + kappa * rmax(zero, zr_arg));
-        icr = one / c_r;
+        icr = rrcp(c_r);
         zl_arg = (pi_r - pi_l) * icr + du;
         c_l = rho_l * (a_l + kappa * rmax(zero, zl_arg));
-        const A sc = c_l + c_r, q = one / (c_l * sc);
+        const A sc = c_l + c_r, q = rrcp(c_l * sc);
         icl = sc * q;
         isum = c_l * q;
     }
@@ -172,7 +172,7 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
         star_right = u <= zero;
         if (star_right) {
             irho = (u_r - u + sr) * icr;
-            rho = one / irho;
+            rho = rrcp(irho);
             ic2 = icr * icr;
             const A e = e_r + (pm - pi_r) * (pm + pi_r) * half * ic2;
             rho3 = rho * rho * rho;
@@ -193,7 +193,7 @@ __device__ __forceinline__ void interface_flux_adjoint(const Cell<A> &UL, const 
             Wt.ut = -urho * irr * v_rx;
         } else {
             irho = (u - u_l + sl) * icl;
-            rho = one / irho;
+            rho = rrcp(irho);
             ic2 = icl * icl;
             const A e = e_l + (pm - pi_l) * (pm + pi_l) * half * ic2;
             rho3 = rho * rho * rho;

@@ -78,19 +78,17 @@ struct Variant {
     cudaError_t (*init)(const LaunchConfig &, cudaStream_t);
     cudaError_t (*plan)(const LaunchConfig &, cudaStream_t);
     cudaError_t (*step)(const LaunchConfig &, cudaStream_t, cudaEvent_t *);
+    cudaError_t (*plan_from)(const LaunchConfig &, cudaStream_t, const double *);
 };
 
-const Variant kVariants[] = {
-    {fvm2d::fp64::prepare, fvm2d::fp64::enqueue_init, fvm2d::fp64::enqueue_plan, fvm2d::fp64::enqueue_step},
-    {fvm2d::fp64_strict::prepare, fvm2d::fp64_strict::enqueue_init, fvm2d::fp64_strict::enqueue_plan,
-     fvm2d::fp64_strict::enqueue_step},
-    {fvm2d::fp64_reforder::prepare, fvm2d::fp64_reforder::enqueue_init, fvm2d::fp64_reforder::enqueue_plan,
-     fvm2d::fp64_reforder::enqueue_step},
-    {fvm2d::fp32::prepare, fvm2d::fp32::enqueue_init, fvm2d::fp32::enqueue_plan, fvm2d::fp32::enqueue_step},
-};
+#define FVM2D_VARIANT_ENTRY(ns)                                                                        \
+    {fvm2d::ns::prepare, fvm2d::ns::enqueue_init, fvm2d::ns::enqueue_plan, fvm2d::ns::enqueue_step,     \
+     fvm2d::ns::enqueue_plan_from}
+const Variant kVariants[] = {FVM2D_VARIANT_ENTRY(fp64), FVM2D_VARIANT_ENTRY(fp64_strict),
+                             FVM2D_VARIANT_ENTRY(fp64_reforder), FVM2D_VARIANT_ENTRY(fp32)};
 // the tangent-linear build (dual numbers), used by fvm2d_jvp only
-const Variant kJvp = {fvm2d::jvp::prepare, fvm2d::jvp::enqueue_init, fvm2d::jvp::enqueue_plan,
-                      fvm2d::jvp::enqueue_step};
+const Variant kJvp = FVM2D_VARIANT_ENTRY(jvp);
+#undef FVM2D_VARIANT_ENTRY
 
 using fvm2d::ad::Dual;
 
@@ -739,6 +737,89 @@ int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows)
         rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
+    return FVM2D_OK;
+}
+
+// ---- row slabs on several devices: asynchronous steps ------------------------
+// The calls below enqueue on the handle's stream and return at once; the
+// caller orders its own work (a halo exchange, a max-reduction over the slabs,
+// e.g. NCCL on a torch stream wrapping fvm2d_get_stream's stream) on the same
+// stream, so a slab step never waits on the host.
+
+int fvm2d_get_stream(fvm2d_solver *s, void **stream)
+{
+    if (int rc = check(s)) return rc;
+    if (!stream) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    *stream = static_cast<void *>(s->stream);
+    return FVM2D_OK;
+}
+
+int fvm2d_get_rows_async(fvm2d_solver *s, int j0, int nrows, double *rows)
+{
+    if (int rc = rows_check(s, j0, nrows, rows)) return rc;
+    if (!is_device_pointer(rows)) return fail(FVM2D_ERR_INVALID, "the row buffer must be device memory");
+    if (is_fp32(s->precision))
+        rows_out<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->plane, s->pitch, j0,
+                                                        nrows, s->nx, rows);
+    else
+        rows_out<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    CK(cudaGetLastError());
+    return FVM2D_OK;
+}
+
+int fvm2d_set_rows_async(fvm2d_solver *s, int j0, int nrows, const double *rows)
+{
+    if (int rc = rows_check(s, j0, nrows, rows)) return rc;
+    if (!is_device_pointer(rows)) return fail(FVM2D_ERR_INVALID, "the row buffer must be device memory");
+    if (is_fp32(s->precision))
+        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, j0, nrows,
+                                                       s->nx, rows);
+    else
+        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    CK(cudaGetLastError());
+    return FVM2D_OK;
+}
+
+int fvm2d_slab_begin(fvm2d_solver *s, double *smax_out)
+{
+    Range range_("fvm2d_slab_begin");
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (!smax_out || !is_device_pointer(smax_out)) return fail(FVM2D_ERR_INVALID, "smax_out must be device memory");
+    StepControl *c = s->ctl_h;
+    std::memset(c, 0, sizeof(StepControl));
+    c->step_limit = INT_MAX;
+    if (int rc = s->upload_control()) return rc;
+    if (int rc = s->build_graphs()) return rc;
+    CK(kVariants[s->precision].init(s->config(), s->stream));
+    s->need_init = false;
+    CK(cudaMemcpyAsync(smax_out, &s->ctl->smax_last, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    return FVM2D_OK;
+}
+
+int fvm2d_slab_step(fvm2d_solver *s, const double *smax_in, double *smax_out)
+{
+    if (int rc = check(s)) return rc;
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    if (!smax_in || !smax_out || !is_device_pointer(smax_in) || !is_device_pointer(smax_out))
+        return fail(FVM2D_ERR_INVALID, "smax_in and smax_out must be device memory");
+    if (s->graph_variant != s->precision || !s->graph[1])
+        return fail(FVM2D_ERR_STATE, "fvm2d_slab_begin must come first (and again after a setter)");
+    CK(kVariants[s->precision].plan_from(s->config(), s->stream, smax_in));
+    CK(cudaGraphLaunch(s->graph[1], s->stream));
+    CK(cudaMemcpyAsync(smax_out, &s->ctl->smax_last, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    s->total_steps += 1;
+    return FVM2D_OK;
+}
+
+int fvm2d_slab_sync(fvm2d_solver *s, double *t, int *steps, int *done)
+{
+    if (int rc = check(s)) return rc;
+    CK(cudaMemcpyAsync(s->ctl_h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (t) *t = s->ctl_h->t;
+    if (steps) *steps = s->ctl_h->steps;
+    if (done) *done = s->ctl_h->done;
     return FVM2D_OK;
 }
 

@@ -58,6 +58,7 @@ constexpr int kStepKernels = 5;
     cudaError_t prepare();                                                     \
     cudaError_t enqueue_init(const LaunchConfig &c, cudaStream_t s);           \
     cudaError_t enqueue_plan(const LaunchConfig &c, cudaStream_t s);           \
+    cudaError_t enqueue_plan_from(const LaunchConfig &c, cudaStream_t s, const double *smax); \
     cudaError_t enqueue_step(const LaunchConfig &c, cudaStream_t s, cudaEvent_t *ev); \
     }
 

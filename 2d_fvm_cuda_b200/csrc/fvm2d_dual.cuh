@@ -62,6 +62,10 @@ __device__ __forceinline__ Dual lane_down(Dual a)
 {
     return Dual(__shfl_down_sync(0xffffffffu, a.v, 1), __shfl_down_sync(0xffffffffu, a.d, 1));
 }
+__device__ __forceinline__ Dual lane_last(Dual a)
+{
+    return Dual(__shfl_sync(0xffffffffu, a.v, 31), __shfl_sync(0xffffffffu, a.d, 31));
+}
 __device__ __forceinline__ Dual lane_up(Dual a)
 {
     return Dual(__shfl_up_sync(0xffffffffu, a.v, 1), __shfl_up_sync(0xffffffffu, a.d, 1));

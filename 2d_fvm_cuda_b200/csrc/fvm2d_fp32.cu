@@ -9,6 +9,8 @@
 #define FVM2D_REAL float
 #define FVM2D_PHYS PackedCompensated
 #define FVM2D_TAPED_STEP  // also the taped step of FP32 differentiation runs
+// the FP64 wave speed from reciprocal square roots (fvm2d_math.cuh)
+#define FVM2D_FAST_RCP
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to
 #ifdef FVM2D_TUNE_X

@@ -5,6 +5,9 @@
 #define FVM2D_REAL double
 #define FVM2D_PHYS Hoisted
 #define FVM2D_TAPED_STEP  // also the taped step of the differentiation form
+// reciprocals and reciprocal square roots from the hardware seeds and one
+// third-order refinement (rrcp/rrsqrt in fvm2d_math.cuh)
+#define FVM2D_FAST_RCP
 // resident sweep blocks per SM (128 threads each) that the register
 // budget is fitted to; measured best for this build at 4096^2
 #ifdef FVM2D_TUNE_X

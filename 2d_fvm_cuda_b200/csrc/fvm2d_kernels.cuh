@@ -66,6 +66,17 @@ __global__ void plan_kernel(StepControl *c, PlanParams p)
     if (threadIdx.x == 0 && blockIdx.x == 0) plan_step(c, p);
 }
 
+// A row slab of a problem split across devices plans its step from the
+// wave-speed maximum over all slabs, which the caller's reduction left in
+// device memory, so no slab waits on the host between steps.
+__global__ void plan_from_kernel(StepControl *c, PlanParams p, const double *smax)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        c->smax_last = *smax;
+        plan_step(c, p);
+    }
+}
+
 // Block-wide max of a non-negative double, folded into *bits with one atomic
 // per block.  Values that are NaN never win (the running max ignores them).
 template <int NT>
@@ -167,11 +178,14 @@ __global__ void __launch_bounds__(NT) init_kernel(Field<Real> U, int nx, int ny,
 // never holds others back.  Both walk the array with a grid-stride loop over
 // work items; the grid is sized to the kernel's occupancy.
 //
-// x-sweep: a work item is 32 consecutive cells of one row.  Lane k holds cell
-// c = 1 + 30*seg + k: it loads cells c-1..c+1, computes the limited slope of
-// c, takes the slope of c-1 from lane k-1 by shuffle and computes the
-// interface c-1/2 (lanes 1..31), then takes the flux of c+1/2 from lane k+1 to
-// update cell c (lanes 1..30).  Items advance by 30 cells.
+// x-sweep: a work item is a segment of one row, walked by a warp in chunks
+// of 32 consecutive cells.  In a chunk lane k holds cell c: it loads cells
+// c-1..c+1 (coalesced), computes the limited slope of c, takes the slope of
+// c-1 from lane k-1 by shuffle and computes the interface c-1/2, then takes
+// the flux of c-3/2 from lane k-1 and updates cell c-1.  Lane 0 takes the
+// slope and flux it needs from lane 31 of the previous chunk, so after the
+// first chunk every lane of every chunk does useful work (in the first chunk
+// lanes 0 and 1 only feed their neighbours).
 //
 // y-sweep: a work item is 32 consecutive columns times one segment of T
 // interfaces along y.  Each lane walks its column in line order (line
@@ -217,11 +231,14 @@ __device__ __forceinline__ void store_cell(const Field<Real> &F, int x, int y, i
     F.at(ft, x, y) = c.ut;
 }
 
-// Value of the next (lane_down) or previous (lane_up) lane of the warp.
+// Value of the next (lane_down) or previous (lane_up) lane of the warp, or of
+// its last lane (lane_last).
 __device__ __forceinline__ double lane_down(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ float lane_down(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ double lane_up(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ float lane_up(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double lane_last(double v) { return __shfl_sync(0xffffffffu, v, 31); }
+__device__ __forceinline__ float lane_last(float v) { return __shfl_sync(0xffffffffu, v, 31); }
 
 template <typename Real>
 __device__ __forceinline__ Cell<Real> shfl_down(const Cell<Real> &c)
@@ -245,9 +262,25 @@ __device__ __forceinline__ Cell<Real> shfl_up(const Cell<Real> &c)
     return o;
 }
 
-// Cells updated per x-sweep work item: lane k holds cell c = 1 + 30 seg + k;
-// lanes 1..31 own the interface c-1/2, lanes 1..30 update cell c.
-constexpr int kXCells = 30;
+template <typename Real>
+__device__ __forceinline__ Cell<Real> shfl_last(const Cell<Real> &c)
+{
+    Cell<Real> o;
+    o.rho = lane_last(c.rho);
+    o.p = lane_last(c.p);
+    o.un = lane_last(c.un);
+    o.ut = lane_last(c.ut);
+    return o;
+}
+
+// Chunks of 32 cells per x-sweep work item, and the cells an item updates:
+// item seg starts at cell b0 = 1 + kXCells seg (lane 0 of its first chunk)
+// and updates cells b0+1 .. b0+kXCells.
+#ifndef FVM2D_X_CHUNKS
+#define FVM2D_X_CHUNKS 4
+#endif
+constexpr int kXChunks = FVM2D_X_CHUNKS;
+constexpr int kXCells = 32 * kXChunks - 2;
 
 // One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
 // wave speed of the interior cells written by a final sweep, and bad whether
@@ -258,18 +291,9 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
                                        int nseg, int lane, double &vmax, int &bad)
 {
     const int nx = a.nx, ny = a.ny;
-    const int c = 1 + seg * kXCells + lane;
-    const bool upd = lane >= 1 && lane <= kXCells && c <= nx - 3;
+    const int b0 = 1 + seg * kXCells;
+    const int last = min(b0 + kXCells, nx - 3);  // last cell this item updates
     auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
-    const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
-    Cell<Real> A;
-    if (FINAL) A = load_cell(a.comb, min(c, nx - 1), y, 2, 3);  // branch A, loaded early
-    const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);          // slope of cell c
-    const Cell<Real> sm1 = shfl_up(s0);                          // slope of cell c-1
-    Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
-    if (lane >= 1 && c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);
-    if (TAPE && lane >= 1 && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // interface c-1/2 at cell c
-    const Cell<Real> FR = shfl_down(F);
     auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
         if (FINAL) {
             Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
@@ -286,7 +310,26 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
             store_cell(a.dst, x, y, 2, 3, U);
         }
     };
-    if (upd) emit(c, Phys::update(c0, F, FR, K), A);
+    Cell<Real> cs = {Real(0), Real(0), Real(0), Real(0)}, cF = cs;  // lane 31's slope and flux, previous chunk
+    for (int j = 0; j < kXChunks; ++j) {
+        const int b = b0 + 32 * j;
+        if (b - 1 > last) break;  // nothing left to update (the same for the whole warp)
+        const int c = b + lane, u = c - 1;  // this lane's cell, and the cell it updates
+        const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
+        Cell<Real> A;
+        if (FINAL) A = load_cell(a.comb, min(max(u, 0), nx - 1), y, 2, 3);  // branch A, loaded early
+        const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);                // slope of cell c
+        Cell<Real> sm1 = shfl_up(s0);                                     // slope of cell c-1
+        if (lane == 0) sm1 = cs;
+        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
+        if (c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);   // interface c-1/2
+        if (TAPE && (j > 0 || lane >= 1) && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // at cell c
+        Cell<Real> FL = shfl_up(F);                                       // interface c-3/2
+        if (lane == 0) FL = cF;
+        if ((j > 0 || lane >= 2) && u <= last) emit(u, Phys::update(cm1, FL, F, K), A);
+        cs = shfl_last(s0);
+        cF = shfl_last(F);
+    }
     // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
     if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
         const int x = seg == 0 ? lane : nx - 2 + lane;
@@ -325,9 +368,48 @@ __host__ __device__ __forceinline__ int y_segments(int ny, int T) { return (ny -
 
 // One y-sweep work item: columns 32 cw .. 32 cw + 31, segment seg (of nseg)
 // of T interfaces.  A TAPE sweep also stores every interface flux.
-template <typename Real, class Phys, bool TAPE = false>
+//
+// RING = 0: the walker keeps its three cells, the next one (loaded one
+// interface ahead), the last slope and the last flux in registers.
+// RING = D > 0: each lane streams its column through a ring of kYRingRows
+// rows in shared memory (`ring`, rows of 4 fields, consecutive entries
+// `rs` elements apart, one column per thread), filled by asynchronous
+// global->shared copies issued D rows ahead of use and waited for per
+// thread (cp.async groups: no barrier, no other thread involved); the
+// registers then hold only the last slope and flux across the Riemann
+// solver, and the loads never stall the walker.
+constexpr int kYRingRows = 8;
+
+template <typename Real>
+__device__ __forceinline__ void async_copy(Real *dst_shared, const Real *src)
+{
+#if defined(__CUDA_ARCH__)
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst_shared);
+    if constexpr (sizeof(Real) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(src) : "memory");
+#else
+    *dst_shared = *src;  // host builds of this file (tests): a plain copy
+#endif
+}
+__device__ __forceinline__ void async_commit()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.commit_group;" ::: "memory");
+#endif
+}
+template <int N>
+__device__ __forceinline__ void async_wait()
+{
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+#endif
+}
+
+template <typename Real, class Phys, bool TAPE = false, int RING = 0>
 __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int seg, int nseg,
-                                       int cw, int lane, int T)
+                                       int cw, int lane, int T, Real *ring = nullptr, int rs = 0)
 {
     const int nx = a.nx, ny = a.ny;
     const int x = cw * 32 + lane;
@@ -336,20 +418,64 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
     const int l0 = 2 + seg * (T - 1);
     const int lend = min(l0 + T - 1, ny - 2);  // last interface of the segment
     auto ld = [&](int l) { return load_cell(a.src, xc, ny - 1 - l, 3, 2); };
-    Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
-    Cell<Real> sm1 = Phys::slope(ld(l0 - 2), cm1, c0, K);
-    Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
-    for (int l = l0; l <= lend; ++l) {
-        const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
-        const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
-        const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
-        if (TAPE && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);  // interface l-1/2 at line position l
-        if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
-        Fp = F;
-        cm1 = c0;
-        c0 = cp1;
-        cp1 = cp2;
-        sm1 = s0;
+    if constexpr (RING == 0) {
+        Cell<Real> cm1 = ld(l0 - 1), c0 = ld(l0), cp1 = ld(l0 + 1);
+        Cell<Real> sm1 = Phys::slope(ld(l0 - 2), cm1, c0, K);
+        Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
+        for (int l = l0; l <= lend; ++l) {
+            const Cell<Real> cp2 = ld(min(l + 2, ny - 1));  // next iteration's cell, loaded one interface ahead
+            const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
+            const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+            if (TAPE && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);  // interface l-1/2 at line position l
+            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
+            Fp = F;
+            cm1 = c0;
+            c0 = cp1;
+            cp1 = cp2;
+            sm1 = s0;
+        }
+    } else {
+        static_assert(RING >= 1 && RING + 3 <= kYRingRows, "prefetch distance does not fit the ring");
+        // row l of the line (clamped to the array) into its ring slot, fields (rho, p, un, ut)
+        auto issue = [&](int l) {
+            const int y = ny - 1 - min(l, ny - 1);
+            Real *r = ring + (l & (kYRingRows - 1)) * 4 * rs;
+            async_copy(r, &a.src.at(0, xc, y));
+            async_copy(r + rs, &a.src.at(1, xc, y));
+            async_copy(r + 2 * rs, &a.src.at(3, xc, y));
+            async_copy(r + 3 * rs, &a.src.at(2, xc, y));
+        };
+        auto get = [&](int l) {
+            const Real *r = ring + (l & (kYRingRows - 1)) * 4 * rs;
+            Cell<Real> c;
+            c.rho = r[0];
+            c.p = r[rs];
+            c.un = r[2 * rs];
+            c.ut = r[3 * rs];
+            return c;
+        };
+        for (int l = l0 - 2; l <= l0 + 1; ++l) issue(l);
+        async_commit();
+        for (int k = 1; k < RING; ++k) {  // rows l0+2 .. l0+RING, one group each
+            issue(l0 + 1 + k);
+            async_commit();
+        }
+        async_wait<RING - 1>();  // rows up to l0+1 have landed
+        Cell<Real> sm1 = Phys::slope(get(l0 - 2), get(l0 - 1), get(l0), K);
+        Cell<Real> Fp = {Real(0), Real(0), Real(0), Real(0)};
+        for (int l = l0; l <= lend; ++l) {
+            issue(l + RING + 1);  // RING rows ahead of the row this iteration needs last
+            async_commit();
+            async_wait<RING>();   // rows up to l+1 have landed
+            const Cell<Real> cm1 = get(l - 1), c0 = get(l), cp1 = get(l + 1);
+            const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
+            const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
+            if (TAPE && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);
+            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(get(l - 1), Fp, F, K));
+            Fp = F;
+            sm1 = s0;
+        }
+        async_wait<0>();  // no copy of this item may land in the ring after it
     }
     // ghost rows pass through (y-sweeps do not update them)
     if (col && seg == 0)
@@ -357,6 +483,10 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
     if (col && seg == nseg - 1)
         for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
 }
+
+#ifndef FVM2D_Y_RING
+#define FVM2D_Y_RING 0
+#endif
 
 template <typename Real, class Phys, int NT, int MINB, bool TAPE = false>
 __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, int T)
@@ -368,8 +498,15 @@ __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, in
     const int nseg = y_segments(a.ny, T);
     const long long nwork = (long long)ncw * nseg;
     const long long wstride = (long long)gridDim.x * (NT / 32);
-    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
-        y_item<Real, Phys, TAPE>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T);
+    constexpr int RING = (sizeof(Real) == 4 || sizeof(Real) == 8) ? FVM2D_Y_RING : 0;
+    if constexpr (RING > 0) {
+        __shared__ Real ring[kYRingRows * 4 * NT];
+        for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+            y_item<Real, Phys, TAPE, RING>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T, ring + threadIdx.x, NT);
+    } else {
+        for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+            y_item<Real, Phys, TAPE>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T);
+    }
 }
 
 // ---------------------------------------------------------------------------

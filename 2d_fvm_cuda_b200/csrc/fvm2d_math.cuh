@@ -36,10 +36,64 @@ __device__ __forceinline__ Real rmax(Real a, Real b) { return (a < b) ? b : a; }
 // argument is NaN)
 __device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
-// 1/sqrt(x): CUDA's rsqrt (1 ulp) and rsqrtf (2 ulp); the dual-number
-// overload lives with the dual type
+// 1/x and 1/sqrt(x).
+//
+// Builds that define FVM2D_FAST_RCP (the FP64 product build, and the FP64
+// wave speed of the FP32 build) take the hardware's approximate seeds --
+// PTX rcp.approx.ftz.f64 and rsqrt.approx.ftz.f64, about 20 correct bits --
+// and refine each by one third-order step (Householder's method of order 3),
+// written from the series
+//   1/x       = r / (1 - e)       = r (1 + e + e^2 + ...),         e = 1 - x r
+//   1/sqrt(x) = y / sqrt(1 - e)   = y (1 + e/2 + 3 e^2/8 + ...),   e = 1 - x y^2
+// truncated after the quadratic term: the relative error falls from about
+// 2^-20 to about 2^-58, below the rounding of the result, so the results are
+// within a couple of ulp of correctly rounded ones (not bit-identical: that
+// build is held to the reference within a relative L1 tolerance).  Each costs
+// the seed and three to five FP64 operations instead of a full IEEE division
+// or square-root sequence.  Other builds use IEEE division and CUDA's rsqrt
+// (1 ulp); rsqrtf is within 2 ulp; the dual-number overloads live with the
+// dual type, and other number types divide.
+#if defined(FVM2D_FAST_RCP)
+__device__ __forceinline__ double rcp_seed(double x)
+{
+#if defined(__CUDA_ARCH__)
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+#else
+    return double(1.0f / float(x));  // host builds of this file (tests): a single-precision seed
+#endif
+}
+__device__ __forceinline__ double rsqrt_seed(double x)
+{
+#if defined(__CUDA_ARCH__)
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+#else
+    return double(1.0f / sqrtf(float(x)));
+#endif
+}
+__device__ __forceinline__ double rrcp(double x)
+{
+    const double r = rcp_seed(x);
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+}
+__device__ __forceinline__ double rrsqrt(double x)
+{
+    const double y = rsqrt_seed(x);
+    const double e = fma(-(x * y), y, 1.0);
+    return fma(y, e * fma(e, 0.375, 0.5), y);
+}
+#else
+__device__ __forceinline__ double rrcp(double x) { return 1.0 / x; }
 __device__ __forceinline__ double rrsqrt(double x) { return ::rsqrt(x); }
+#endif
+__device__ __forceinline__ float rrcp(float x) { return 1.0f / x; }
 __device__ __forceinline__ float rrsqrt(float x) { return ::rsqrtf(x); }
+template <typename Real>
+__device__ __forceinline__ Real rrcp(Real x) { return Real(1) / x; }
 
 // Generalized-minmod slope of one component from its left (m), centre (c)
 // and right (p) values.  src/basicFuns.cuh:49-68.
@@ -332,7 +386,7 @@ struct Hoisted {
         const Real rho_rx = sR.rho, pi_rx = sR.p, u_rx = sR.un, v_rx = sR.ut;
 
         // 1/rho_l and 1/rho_r from one division
-        const Real irlr = one / (rho_l * rho_r);
+        const Real irlr = rrcp(rho_l * rho_r);
         const Real irl = rho_r * irlr, irr = rho_l * irlr;
         const Real e_l = pi_l * irl * igm1, e_r = pi_r * irr * igm1;
         const Real e_lx = (pi_lx - pi_l * rho_lx * irl) * irl * igm1;
@@ -349,16 +403,16 @@ struct Hoisted {
         Real c_l, c_r, icl, icr, isum;
         if (pi_r >= pi_l) {
             c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) * ir + du));
-            icl = one / c_l;
+            icl = rrcp(c_l);
             c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) * icl + du));
-            const Real sc = c_l + c_r, q = one / (c_r * sc);
+            const Real sc = c_l + c_r, q = rrcp(c_r * sc);
             icr = sc * q;
             isum = c_r * q;
         } else {
             c_r = rho_r * (a_r + kappa * rmax(zero, (pi_l - pi_r) * il + du));
-            icr = one / c_r;
+            icr = rrcp(c_r);
             c_l = rho_l * (a_l + kappa * rmax(zero, (pi_r - pi_l) * icr + du));
-            const Real sc = c_l + c_r, q = one / (c_l * sc);
+            const Real sc = c_l + c_r, q = rrcp(c_l * sc);
             icl = sc * q;
             isum = c_l * q;
         }
@@ -390,7 +444,7 @@ struct Hoisted {
             o.un = u;
             if (u <= zero) {
                 const Real irho = (u_r - u + sr) * icr;
-                const Real rho = one / irho;
+                const Real rho = rrcp(irho);
                 const Real icr2 = icr * icr;
                 const Real e = e_r + (pm - pi_r) * (pm + pi_r) * half * icr2;
                 const Real rho3 = rho * rho * rho, urho = u * rho;
@@ -403,7 +457,7 @@ struct Hoisted {
                 o.ut_t = -urho * irr * v_rx;
             } else {
                 const Real irho = (u - u_l + sl) * icl;
-                const Real rho = one / irho;
+                const Real rho = rrcp(irho);
                 const Real icl2 = icl * icl;
                 const Real e = e_l + (pm - pi_l) * (pm + pi_l) * half * icl2;
                 const Real rho3 = rho * rho * rho, urho = u * rho;
@@ -462,7 +516,7 @@ struct Hoisted {
         m1 -= (FR.p - FL.p) * K.lambda;
         m2 -= (FR.un - FL.un) * K.lambda;
         m3 -= (FR.ut - FL.ut) * K.lambda;
-        const Real ir = Real(1) / m0;
+        const Real ir = rrcp(m0);
         Cell<Real> o;
         o.rho = m0;
         o.un = m1 * ir;
@@ -549,9 +603,20 @@ template <typename Real>
 __device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, double g)
 {
     double du = double(u), dv = double(v);
+#if defined(FVM2D_FAST_RCP)
+    // sqrt(q) = q / sqrt(q) and sqrt(g p / rho) = |g p| / sqrt(g p rho):
+    // two reciprocal square roots, no division; states where g p rho is not
+    // positive (invalid ones) take the reference's expression
+    const double q = du * du + dv * dv;
+    const double velo = q > 0.0 ? q * rrsqrt(q) : 0.0;
+    const double gp = g * double(p), gpr = gp * double(rho);
+    const double c = gpr > 0.0 ? fabs(gp) * rrsqrt(gpr) : sqrt(gp / double(rho));
+    return velo + c;
+#else
     double velo = sqrt(du * du + dv * dv);
     double c = sqrt(g * double(p) / double(rho));
     return fabs(velo) + c;
+#endif
 }
 
 } // namespace FVM2D_VARIANT

@@ -55,6 +55,24 @@ def seeded_four_quadrant(nx: int, ny: int, seed: int, split=None) -> np.ndarray:
     return four_quadrant(*seeded_quadrant_states(seed), nx, ny, split)
 
 
+def stacked_four_quadrant_rows(nx: int, tile_ny: int, lo: int, hi: int) -> np.ndarray:
+    """Rows [lo, hi) of seeded four-quadrant tiles of tile_ny rows stacked
+    top to bottom, tile k drawn from seed k (tile k alone is
+    seeded_four_quadrant(nx, tile_ny, k)): one tall problem whose rows can be
+    built slab by slab without the whole array."""
+    U = np.empty((hi - lo, nx, 4))
+    hx = nx // 2
+    for k in range(lo // tile_ny, (hi - 1) // tile_ny + 1):
+        U1, U2, U3, U4 = seeded_quadrant_states(k)
+        a, b = max(lo, k * tile_ny), min(hi, (k + 1) * tile_ny)
+        mid = k * tile_ny + tile_ny // 2
+        top = slice(a - lo, max(a, min(b, mid)) - lo)
+        bot = slice(max(a, min(b, mid)) - lo, b - lo)
+        U[top, :hx], U[top, hx:] = U2[:4], U1[:4]
+        U[bot, :hx], U[bot, hx:] = U3[:4], U4[:4]
+    return U
+
+
 def uneven_batch(count: int, seed: int, sizes=tuple(range(128, 1025, 64))):
     """`count` seeded four-quadrant problems for the batched form: per-side
     size drawn from `sizes`, split point ~U[0.3, 0.7]^2, states as

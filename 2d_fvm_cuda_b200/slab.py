@@ -20,6 +20,15 @@ Every rank computes exactly the cells a single device would, with the same
 arithmetic and the same dt, so the gathered result equals a single-device
 run bit for bit.  With the NCCL backend the halo rows travel between device
 buffers; with any other backend through host memory.
+
+With NCCL and the library's solver handle the steps never wait on the host:
+the rows are packed and unpacked, the halos exchanged, the wave-speed maximum
+reduced (8 bytes, on the device) and the next step planned from it by a
+kernel, all enqueued in order on the handle's own CUDA stream (NCCL runs on
+a torch stream wrapping it).  The host reads the time back only when asked
+(``sync``) or every few steps of ``solve``.  Other backends, or a stand-in
+solver, take the host-driven path (``step``): the maximum read back to the
+host and the dt computed there.
 """
 from __future__ import annotations
 
@@ -78,20 +87,29 @@ class SlabSolver:
     """This rank's part of a problem of ny x nx cells (ghost layers included).
 
     ``U`` is the whole initial state, shape (ny, nx, 4|5), on every rank (each
-    keeps its rows).  ``make_local(nx, rows)`` builds the rank's solver (a
-    ``Handle`` by default); ``group`` is the process group (default: WORLD).
+    keeps its rows), or a function ``U(lo, hi)`` returning global rows
+    [lo, hi) of it, in which case ``shape`` = (ny, nx) gives the problem's
+    size.  ``make_local(nx, rows)`` builds the rank's solver (a ``Handle`` by
+    default); ``group`` is the process group (default: WORLD).
     """
 
     def __init__(self, U, width=1.0, height=1.0, t_end=0.0, cfl=0.5, alpha=1.9, gamma=1.4, strategy=OUTFLOW,
-                 precision=0, group=None, make_local=None):
+                 precision=0, group=None, make_local=None, shape=None):
         import torch.distributed as dist
 
         self.dist = dist
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
-        U = np.asarray(U, dtype=np.float64)
-        self.ny, self.nx = U.shape[:2]
+        if callable(U):
+            if shape is None:
+                raise ValueError("shape=(ny, nx) is required when U is a function of the rows")
+            self.ny, self.nx = int(shape[0]), int(shape[1])
+            rows_of = U
+        else:
+            U = np.asarray(U, dtype=np.float64)
+            self.ny, self.nx = U.shape[:2]
+            rows_of = lambda lo, hi: U[lo:hi]  # noqa: E731
         self.strategy = int(strategy)
         self.l_lo, self.l_hi = local_rows(self.ny, self.world, self.rank)
         self.lo, self.hi = plan_slabs(self.ny, self.world)[self.rank]
@@ -108,10 +126,19 @@ class SlabSolver:
         self.local.configure(width, height, t_end, cfl, alpha, gamma, self.strategy, precision)
         row0, gny, top, bottom = row_frame(self.ny, self.world, self.rank, self.strategy)
         self.local.set_row_frame(row0, gny, top, bottom)
-        self.local.set_state(np.ascontiguousarray(U[self.l_lo:self.l_hi]))
+        self.local.set_state(np.ascontiguousarray(rows_of(self.l_lo, self.l_hi), dtype=np.float64))
         self.device = dist.get_backend(group) == "nccl"
         self.msgs = halo_messages(self.ny, self.world, self.strategy)
         self._bufs = [self._buffer() for _ in self.msgs]
+        # steps enqueued on the device, no host round trip (NCCL + the library's handle)
+        self.on_device = self.device and hasattr(self.local, "slab_step")
+        if self.on_device:
+            import torch
+
+            self._stream = torch.cuda.ExternalStream(self.local.stream_ptr())
+            self._smax_local = torch.zeros(1, dtype=torch.float64, device="cuda")
+            self._smax_all = torch.zeros(1, dtype=torch.float64, device="cuda")
+            self._begun = False
 
     # ---- buffers -------------------------------------------------------------
     def _buffer(self, rows=HALO):
@@ -140,6 +167,15 @@ class SlabSolver:
 
     def _global(self, r: int) -> int:
         return self.dist.get_global_rank(self.group, r) if self.group is not None else r
+
+    def set_local_state(self, R) -> None:
+        """Replaces this rank's rows (its slab and halo rows: global rows
+        l_lo .. l_hi-1, shape (l_hi - l_lo, nx, 4|5), host or pinned memory)
+        and restarts the run at t = 0."""
+        self.local.set_state(R)
+        self.t, self.steps, self.done, self.fresh = 0.0, 0, False, True
+        if self.on_device:
+            self._begun = False
 
     # ---- one step ------------------------------------------------------------
     def exchange(self) -> None:
@@ -170,8 +206,57 @@ class SlabSolver:
         self.dist.all_reduce(v, op=self.dist.ReduceOp.MAX, group=self.group)
         return float(v.item())
 
+    # ---- steps enqueued on the device (NCCL) --------------------------------------
+    def _exchange_on_stream(self) -> None:
+        """The halo exchange, enqueued on the handle's stream (the caller has
+        made it torch's current stream)."""
+        dist = self.dist
+        ops, recvs = [], []
+        for k, (src, dst, g_send, g_recv) in enumerate(self.msgs):
+            buf = self._bufs[k]
+            if src == self.rank:
+                self.local.get_rows_async(g_send - self.l_lo, HALO, buf.data_ptr())
+                ops.append(dist.P2POp(dist.isend, buf, self._global(dst), self.group, k))
+            elif dst == self.rank:
+                ops.append(dist.P2POp(dist.irecv, buf, self._global(src), self.group, k))
+                recvs.append((g_recv, buf))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()  # NCCL: the stream waits, the host does not
+        for g_recv, buf in recvs:
+            self.local.set_rows_async(g_recv - self.l_lo, HALO, buf.data_ptr())
+
+    def enqueue_steps(self, n: int) -> None:
+        """Enqueues n steps of the whole problem (NCCL path); returns without
+        waiting.  Steps after the loop has ended do nothing."""
+        import torch
+
+        with torch.cuda.stream(self._stream):
+            for _ in range(n):
+                if not self._begun:
+                    self.local.slab_begin(self._smax_local.data_ptr())
+                    self._begun = True
+                elif not self.fresh:
+                    self._exchange_on_stream()
+                self._smax_all.copy_(self._smax_local)
+                self.dist.all_reduce(self._smax_all, op=self.dist.ReduceOp.MAX, group=self.group)
+                self.local.slab_step(self._smax_all.data_ptr(), self._smax_local.data_ptr())
+                self.fresh = False
+
+    def sync(self) -> tuple[float, int, bool]:
+        """Waits for the enqueued steps; (t, steps, done).  Every rank reaches
+        the same values (the same dt everywhere)."""
+        self.t, self.steps, self.done = self.local.slab_sync()
+        return self.t, self.steps, self.done
+
     def step(self) -> bool:
         """One step of the whole problem; False once the loop has ended."""
+        if self.on_device:
+            if self.done:
+                return False
+            before = self.steps
+            self.enqueue_steps(1)
+            return self.sync()[1] > before
         if self.done:
             return False
         if not self.fresh:
@@ -193,12 +278,22 @@ class SlabSolver:
         return True
 
     def advance(self, n: int) -> int:
+        if self.on_device:
+            before = self.steps
+            self.enqueue_steps(n)
+            return self.sync()[1] - before
         k = 0
         while k < n and self.step():
             k += 1
         return k
 
-    def solve(self) -> int:
+    def solve(self, check_every: int = 16) -> int:
+        if self.on_device:
+            before = self.steps
+            while not self.done:
+                self.enqueue_steps(check_every)
+                self.sync()
+            return self.steps - before
         k = 0
         while self.step():
             k += 1
@@ -209,7 +304,14 @@ class SlabSolver:
         """This rank's rows [lo, hi) of the state, shape (hi-lo, nx, 4); the
         wrapped ghost rows of a periodic run are refreshed first.  Collective."""
         if not self.fresh:
-            self.exchange()
+            if self.on_device:
+                import torch
+
+                with torch.cuda.stream(self._stream):
+                    self._exchange_on_stream()
+                self.sync()
+            else:
+                self.exchange()
             self.fresh = True
         R = self.local.get_rows(self.lo - self.l_lo, self.hi - self.lo)
         return np.ascontiguousarray(np.moveaxis(R, 0, -1))

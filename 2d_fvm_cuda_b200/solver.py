@@ -32,6 +32,24 @@ class precision(enum.IntEnum):
     fp32 = _lib.FP32                    # FP32 storage/arithmetic, compensated update, FP64 dt
 
 
+def write_matrix_txt(dir: str, U, t: float) -> None:
+    """src/wrappers.cuh:370-397 (writeMatrixTo_txt): rho_/p_/u_/v_<t>s.txt in
+    `dir`, the time formatted as std::to_string(double) does ("%f"), one text
+    row per grid row of U (ny, nx, 4|5), each value in the default stream
+    format (6 significant digits, "%g") followed by a space."""
+    tag = "%f" % t
+    names = ("rho", "p", "u", "v")
+    files = [open(os.path.join(dir, f"{n}_{tag}s.txt"), "w") for n in names]
+    try:
+        for row in U:
+            for k, f in enumerate(files):
+                f.write("".join("%g " % x for x in row[:, k]))
+                f.write("\n")
+    finally:
+        for f in files:
+            f.close()
+
+
 class RGRP_2D_CUDA:
     """Split 2D Euler solver: MUSCL + generalized minmod + relaxation GRP.
 
@@ -136,22 +154,11 @@ class RGRP_2D_CUDA:
         return self._stages
 
     def writeFinalResultTo_txt(self, dir: str) -> None:
-        """rho_/p_/u_/v_<endTime>s.txt, one text row per grid row, values in
-        the default 6-significant-digit format followed by a space
-        (src/wrappers.cuh:318-321, 370-397)."""
+        """rho_/p_/u_/v_<endTime>s.txt of the last result
+        (src/wrappers.cuh:318-321); see write_matrix_txt."""
         if self._U is None:
             return
-        tag = "%f" % self._end_time  # std::to_string(double)
-        names = ("rho", "p", "u", "v")
-        files = [open(os.path.join(dir, f"{n}_{tag}s.txt"), "w") for n in names]
-        try:
-            for row in self._U:
-                for k, f in enumerate(files):
-                    f.write("".join("%g " % x for x in row[:, k]))
-                    f.write("\n")
-        finally:
-            for f in files:
-                f.close()
+        write_matrix_txt(dir, self._U, self._end_time)
 
     def clear(self) -> None:
         """src/wrappers.cuh:347-353."""

@@ -24,8 +24,10 @@ product arm (default):
               (oracle/_ref/libref_host.so) on all host cores, bounded sample
   reference_cuda  the reference's own CUDA kernels (oracle/_ref/ref_gpu) on
               the same GPU and workload, timed by its own loop timer
-N > 1: independent replicas, one per GPU (the four-quadrant problems share
-nothing), weak scaling, max-over-ranks device time.
+N > 1: one problem in row slabs, one per GPU (2d_fvm_cuda_b200/slab.py over
+NCCL): the N = 1 workload's tiles stacked into a 4096 x 4096N array, every
+step a halo exchange and a max all-reduce enqueued with the kernels on the
+solver's stream; weak scaling, max-over-ranks device time.
 
 reference arm (--impl reference): rank 0 times the reference's own kernels
 on the host cores (oracle/_ref/libref_host.so; the C oracle if that build is
@@ -118,8 +120,8 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def dist_setup(world, local_rank):
-    if world <= 1:
+def dist_setup(world, local_rank, force=False):
+    if world <= 1 and not force:
         return None
     import datetime
     import torch
@@ -342,6 +344,92 @@ def product_arm(args, rank, world, local_rank):
     return out
 
 
+def slab_arm(args, rank, world, local_rank):
+    """N > 1: one problem cut into row slabs, one per GPU (2d_fvm_cuda_b200/slab.py
+    over NCCL): the four-quadrant tiles of the N = 1 workload stacked into a
+    4096 x 4096 N array on [0,1] x [0,N] (tile k seeded with k), so each GPU
+    keeps the N = 1 workload's cells (weak scaling).  Every step exchanges two
+    halo rows with each neighbour (NCCL send/recv of device buffers) and
+    all-reduces the 8-byte wave-speed max; both are enqueued on the solver's
+    stream with the step kernels, so no step waits on the host."""
+    import torch
+
+    dist = dist_setup(world, local_rank, force=True)
+    pkg = importlib.import_module("2d_fvm_cuda_b200")
+    n = args.n
+    ny = n * world
+    rows = lambda lo, hi: pkg.scenarios.stacked_four_quadrant_rows(n, n, lo, hi)  # noqa: E731
+    kw = dict(width=CFG["width"], height=CFG["height"] * world, t_end=CFG["t_end"], cfl=CFG["cfl"],
+              alpha=CFG["alpha"], gamma=CFG["gamma"], strategy=CFG["strategy"])
+    S = pkg.slab.SlabSolver(rows, shape=(ny, n), precision=pkg.FP64, **kw)
+    assert S.on_device
+    S.advance(args.warmup)
+    stream = torch.cuda.ExternalStream(S.local.stream_ptr())
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    S.advance(8)  # untimed pre-roll while the clock sampler starts
+    barrier(dist)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    before = S.steps
+    e0.record(stream)
+    S.enqueue_steps(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    _, steps_now, _ = S.sync()
+    clocks = sampler.stop()
+    dev_ms = e0.elapsed_time(e1)
+    assert steps_now - before == args.steps, f"only {steps_now - before} of {args.steps} steps ran"
+    barrier(dist)
+    dev_ms_max = allreduce_max(dist, dev_ms)
+    owned = S.hi - S.lo
+    value = n * ny * args.steps / (dev_ms_max / 1e3)
+
+    # e2e through the public API with host buffers: this rank's slab uploaded
+    # from pinned memory, every step enqueued and its control record read
+    # back, the owned rows downloaded at the end
+    pin_in = torch.empty((S.l_hi - S.l_lo, n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    pin_in[:] = rows(S.l_lo, S.l_hi)
+    barrier(dist)
+    t0 = time.perf_counter()
+    S.set_local_state(pin_in)
+    for _ in range(args.steps):
+        S.enqueue_steps(1)
+        S.sync()
+    out_rows = S.owned_rows()
+    e2e_s = allreduce_max(dist, time.perf_counter() - t0)
+    S.close()
+    e2e = n * ny * args.steps / e2e_s
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"four_quadrant_slabs_{n}x{ny}_fp64", "nx": n, "ny": ny,
+                       "rows_per_gpu": owned, "ghost": "outflow", "cfl": CFG["cfl"], "alpha": CFG["alpha"],
+                       "gamma": CFG["gamma"], "seed": "tile k seeded with k",
+                       "arithmetic": "FP64, FMA contraction (nvcc default)",
+                       "l2": "inputs larger than L2 (three 537 MB state buffers per GPU)",
+                       "parallelism": f"row slabs x{world}: NCCL halo exchange (2 rows per neighbour) "
+                                      "+ 8-byte max all-reduce per step, enqueued on the solver stream"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": pin_in.nbytes / args.steps,
+                    "d2h_bytes_per_step": 64 + out_rows.nbytes / args.steps,
+                    "path": "SlabSolver: fvm2d_set_state(pinned slab) + steps x (enqueued step + control read) "
+                            "+ owned rows downloaded"},
+            "clocks": clocks,
+            "gpu_launches": args.steps * (fvm2d_kernels_per_slab_step(world)),
+        }
+    dist.barrier()
+    dist.destroy_process_group()
+    return out
+
+
+def fvm2d_kernels_per_slab_step(world: int) -> int:
+    """The library's kernels per slab step: plan + the 5 step kernels, and a
+    pack (rows out) and unpack (rows in) per halo message of an inner rank."""
+    return 6 + (4 if world > 2 else 2)
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return None
@@ -460,25 +548,36 @@ def adjoint_summary(pkg):
         fwd.append(h.run_stats()[0])
     cot = np.zeros_like(U)
     cot[..., 0] = np.cos(np.arange(n))[None, :]
-    best = None
-    for _ in range(3):
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        h.set_state(U)
-        torch.cuda.synchronize()
-        e0.record()
-        h.forward(steps, pkg.FULL_TAPE)
-        e1.record()
-        h.vjp(cot)
-        e2.record()
-        torch.cuda.synchronize()
-        t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
-        if best is None or sum(t) < sum(best):
-            best = t
+
+    def timed(checkpoints):
+        best = None
+        for _ in range(3):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            h.set_state(U)
+            torch.cuda.synchronize()
+            e0.record()
+            h.forward(steps, checkpoints)
+            e1.record()
+            h.vjp(cot)
+            e2.record()
+            torch.cuda.synchronize()
+            t = (e0.elapsed_time(e1), e1.elapsed_time(e2))
+            if best is None or sum(t) < sum(best):
+                best = t
+        return best
+
+    best = timed(pkg.FULL_TAPE)
+    ck = timed(15)  # ceil(sqrt(200)) checkpoints, each segment recomputed by the VJP
     h.close()
     f = min(fwd[1:])
-    return {"workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, FP64, full tape (11.7 GB)",
-            "forward_ms": f, "taped_forward_ms": best[0], "vjp_ms": best[1],
-            "forward_plus_adjoint_over_forward": sum(best) / f}
+    return {"workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, FP64",
+            "forward_ms": f,
+            "full_tape": {"tape_gb": steps * 7 * 4 * n * n * 8 / 1e9, "taped_forward_ms": best[0],
+                          "vjp_ms": best[1], "forward_plus_adjoint_over_forward": sum(best) / f},
+            "checkpointed": {"checkpoints": 15, "forward_ms": ck[0], "vjp_ms": ck[1],
+                             "forward_plus_adjoint_over_forward": sum(ck) / f},
+            "forward_plus_adjoint_over_forward": sum(best) / f,
+            "checkpointed_ratio": sum(ck) / f}
 
 
 def form_adjoint(args):
@@ -680,6 +779,8 @@ def main():
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="arithmetic of a --kernels-only run")
+    ap.add_argument("--slabs", action="store_true",
+                    help="the row-slab path (the default for N > 1) also on one GPU, under torchrun")
     ap.add_argument("--no-configs", action="store_true",
                     help="leave the FP32 config-1/config-2 error runs out of the default line")
     ap.add_argument("--form", choices=["batch", "adjoint", "vortex", "precision"],
@@ -696,6 +797,8 @@ def main():
         return
     if args.impl == "reference":
         out = reference_arm(args, rank, world)
+    elif (world > 1 or args.slabs) and not args.kernels_only:
+        out = slab_arm(args, rank, world, local_rank)
     else:
         out = product_arm(args, rank, world, local_rank)
     if rank == 0 and out is not None:

@@ -198,6 +198,32 @@ int fvm2d_set_row_frame(fvm2d_solver *s, int row0, int ny_global, int fill_top, 
 int fvm2d_get_rows(fvm2d_solver *s, int j0, int nrows, double *rows);
 int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows);
 
+/* Asynchronous slab steps, for slabs on several devices whose halo exchange
+ * and wave-speed reduction run on the device (NCCL, say): the calls below
+ * only enqueue work on the handle's stream (*stream from fvm2d_get_stream, a
+ * cudaStream_t) and return at once.  The caller enqueues its exchange and
+ * reduction on that same stream between them, so no step waits on the host.
+ *
+ * fvm2d_get_rows_async / fvm2d_set_rows_async: as fvm2d_get_rows /
+ * fvm2d_set_rows, device memory only.
+ * fvm2d_slab_begin: starts a run from t = 0 with no step limit and writes
+ * this slab's wave-speed max of the current state to *smax_out (device
+ * memory, one double).
+ * fvm2d_slab_step: one step whose dt follows the reference's rule
+ * (src/wrappers.cuh:196-207) from *smax_in (device memory: the max over all
+ * slabs of what fvm2d_slab_begin or the previous fvm2d_slab_step wrote) and
+ * the handle's time, then writes this slab's wave-speed max of the new state
+ * to *smax_out.  A step after the loop has ended (the end time reached)
+ * does nothing.
+ * fvm2d_slab_sync: waits for the stream and reads back the time, the steps
+ * taken since fvm2d_slab_begin and whether the loop has ended. */
+int fvm2d_get_stream(fvm2d_solver *s, void **stream);
+int fvm2d_get_rows_async(fvm2d_solver *s, int j0, int nrows, double *rows);
+int fvm2d_set_rows_async(fvm2d_solver *s, int j0, int nrows, const double *rows);
+int fvm2d_slab_begin(fvm2d_solver *s, double *smax_out);
+int fvm2d_slab_step(fvm2d_solver *s, const double *smax_in, double *smax_out);
+int fvm2d_slab_sync(fvm2d_solver *s, double *t, int *steps, int *done);
+
 /* getComputationTime_ms (src/wrappers.cuh:308-311): wall time of the last
  * solve()/advance() loop in milliseconds. */
 int fvm2d_get_computation_time_ms(fvm2d_solver *s, double *ms);
@@ -231,6 +257,14 @@ int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *s
  * The FP64-pipe roofline of the sweeps is quoted against it.  No reference
  * counterpart (diagnostics). */
 int fvm2d_measure_fp64_peak(double *tflops, double *ms_per_launch);
+
+/* The FP64 product build's reciprocal and reciprocal square root (hardware
+ * seeds refined by one third-order step instead of IEEE division and
+ * square root) on n arguments in device memory: rcp[k] ~ 1/x[k],
+ * rsqrt_out[k] ~ 1/sqrt(x[k]).  For tests of their error bound (within a
+ * couple of ulp of the correctly rounded values).  No reference counterpart
+ * (diagnostics). */
+int fvm2d_eval_reciprocals(const double *x, long long n, double *rcp, double *rsqrt_out);
 
 /* ---- differentiation (no reference counterpart) ----------------------------
  * Derivatives of the step with respect to the state, at a fixed step size so

@@ -142,7 +142,10 @@ static inline T __shfl_down_sync(unsigned, T v, int d) { return emu::exchange(v,
 template <typename T>
 static inline T __shfl_up_sync(unsigned, T v, int d) { return emu::exchange(v, -d); }
 template <typename T>
-static inline T __shfl_sync(unsigned, T v, int) { return v; }
+static inline T __shfl_sync(unsigned, T v, int src)
+{
+    return emu::exchange(v, (src & (emu::kLanes - 1)) - emu::flat_thread() % emu::kLanes);
+}
 static inline void __syncthreads() { emu::block_bar.wait(); }
 static inline void __threadfence() {}
 static inline int __any_sync(unsigned, int p) { return emu::vote_any(p); }

@@ -150,11 +150,16 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
         });
     } else {
         const int ncw = (nx + 31) / 32, nseg = y_segments(ny, T);
+        // policy 2: RefOrder items that stream their columns through the
+        // shared-memory ring (one ring per lane, as per thread on the GPU)
+        std::vector<double> ring(kYRingRows * 4 * 32);
         for (int seg = 0; seg < nseg; ++seg)
             for (int cw = 0; cw < ncw; ++cw)
                 for (int lane = 0; lane < 32; ++lane) {
                     if (policy == 0)
                         y_item<double, RefOrder>(a, K, seg, nseg, cw, lane, T);
+                    else if (policy == 2)
+                        y_item<double, RefOrder, false, 4>(a, K, seg, nseg, cw, lane, T, ring.data() + lane, 32);
                     else
                         y_item<double, Hoisted>(a, K, seg, nseg, cw, lane, T);
                 }

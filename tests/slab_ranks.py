@@ -141,3 +141,31 @@ def gpu_worker(rank, world, port, case, out_path):
             np.savez(out_path, G=G, t=S.t, steps=S.steps)
     finally:
         dist.destroy_process_group()
+
+
+def nccl_worker(rank, world, port, case, out_path):
+    """One rank per GPU over NCCL: the steps are enqueued on the device (halo
+    rows packed, exchanged and unpacked on the handle's stream, the wave-speed
+    max reduced on the device and the step planned from it), no host round
+    trip per step.  With one GPU the group has one rank."""
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(rank)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", rank))
+    try:
+        pkg = importlib.import_module("2d_fvm_cuda_b200")
+        U = pkg.scenarios.seeded_four_quadrant(case["nx"], case["ny"], case["seed"])
+        S = pkg.slab.SlabSolver(lambda lo, hi: U[lo:hi], shape=U.shape[:2], width=case["width"],
+                                height=case["height"], t_end=case["t_end"], cfl=0.45, alpha=1.9, gamma=1.4,
+                                strategy=case["strategy"], precision=case["precision"])
+        assert S.on_device
+        k = S.advance(case["first"])  # a fixed number of steps, then the rest of the run in groups
+        S.solve(check_every=5)
+        G = S.gather()
+        S.close()
+        if rank == 0:
+            np.savez(out_path, G=G, t=S.t, steps=S.steps, first=k)
+    finally:
+        dist.destroy_process_group()

@@ -50,12 +50,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CUDA_INC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
 
 
-def build_host(tmp_path_factory, source):
+def build_host(tmp_path_factory, source, defines=()):
     if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INC, "cuda_runtime.h")):
         pytest.skip("needs g++ and the CUDA headers")
     so = str(tmp_path_factory.mktemp("kernels_host") / (os.path.splitext(source)[0] + ".so"))
     subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-pthread",
-                    "-I", CUDA_INC, os.path.join(HERE, source), "-o", so], check=True)
+                    *[f"-D{d}" for d in defines], "-I", CUDA_INC, os.path.join(HERE, source), "-o", so],
+                   check=True)
     return ctypes.CDLL(so)
 
 
@@ -69,9 +70,8 @@ def k32(tmp_path_factory):
     return lib
 
 
-@pytest.fixture(scope="module")
-def kh(tmp_path_factory):
-    lib = build_host(tmp_path_factory, "kernels_host.cpp")
+def _kernels_host(tmp_path_factory, defines=()):
+    lib = build_host(tmp_path_factory, "kernels_host.cpp", defines)
     lib.kh_ghost.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                              ctypes.c_void_p]
@@ -91,7 +91,20 @@ def kh(tmp_path_factory):
     return lib
 
 
-REF, HOISTED = 0, 1
+@pytest.fixture(scope="module")
+def kh(tmp_path_factory):
+    return _kernels_host(tmp_path_factory)
+
+
+@pytest.fixture(scope="module")
+def kh_fast(tmp_path_factory):
+    """The same device code with FVM2D_FAST_RCP, as the FP64 product build is
+    compiled: reciprocals and reciprocal square roots from a seed refined by
+    one third-order step (on the host the seed is a single-precision one)."""
+    return _kernels_host(tmp_path_factory, ("FVM2D_FAST_RCP",))
+
+
+REF, HOISTED, REF_RING = 0, 1, 2
 ALPHA, GAMMA = 1.9, 1.4
 
 
@@ -141,16 +154,19 @@ def test_sweep_items_equal_the_oracle_sweeps(kh, oracle, pkg, nx, ny):
     RY = oracle.sweep_y(U, height, dt)
     for T in (8, 16, 32, 64, 4):  # the kernels choose 64, 32, 16 or 8; 4 for short segments
         assert np.array_equal(sweep(kh, REF, 1, U, height / ny, dt, T), RY), T
+        # the walker that streams its columns through the shared-memory ring
+        assert np.array_equal(sweep(kh, REF_RING, 1, U, height / ny, dt, T), RY), T
 
 
+@pytest.mark.parametrize("fast", [False, True], ids=["ieee_division", "refined_reciprocals"])
 @pytest.mark.parametrize("nx,ny", SWEEP_SIZES[:3])
-def test_hoisted_sweep_items_agree_to_rounding(kh, oracle, pkg, nx, ny):
+def test_hoisted_sweep_items_agree_to_rounding(kh, kh_fast, oracle, pkg, nx, ny, fast):
     U, width, height, dt = sweep_case(pkg, oracle, nx, ny, 4)
     cases = ((0, oracle.sweep_x(U, width, dt), width / nx), (1, oracle.sweep_y(U, height, dt), height / ny))
     for direction, R, h in cases:
-        H = sweep(kh, HOISTED, direction, U, h, dt)
+        H = sweep(kh_fast if fast else kh, HOISTED, direction, U, h, dt)
         rel = np.abs(H - R).max(axis=(0, 1)) / np.abs(R).max(axis=(0, 1))
-        assert rel.max() <= 1e-13, (direction, rel)  # measured 1.5e-16
+        assert rel.max() <= 1e-13, (direction, rel)  # measured 1.5e-16 (IEEE division)
 
 
 def normwise(A, R):

@@ -34,3 +34,10 @@ def test_sedov(pkg):
     U = pkg.scenarios.sedov_1d(16)
     assert U[3, 8, 1] == 0.4 * 3200000.0 / (8.0 / 16) and U[3, 7, 1] == U[3, 8, 1]
     assert U[3, 6, 1] == 0.4 * 1e-12
+
+
+def test_stacked_tiles_built_row_range_by_row_range(pkg):
+    sc = pkg.scenarios
+    A = np.concatenate([sc.seeded_four_quadrant(40, 30, k) for k in range(3)])
+    for lo, hi in [(0, 90), (5, 37), (28, 32), (29, 61), (60, 90), (0, 1), (89, 90), (15, 16)]:
+        assert np.array_equal(sc.stacked_four_quadrant_rows(40, 30, lo, hi), A[lo:hi]), (lo, hi)

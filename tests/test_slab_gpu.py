@@ -3,7 +3,10 @@ its own libfvm2d solver holding a slab plus halo rows, exchanging rows
 through host memory between steps (gloo).  The gathered result must equal a
 single solver's run of the whole array bit for bit, including the presets
 whose ghost rules use global row numbers (jet rows, the double-Mach shock
-position)."""
+position).  The NCCL path, whose steps are enqueued on the device with no
+host round trip (asynchronous row transfers, device-side max reduction and
+step plan), runs as one rank on the one GPU and must equal the single
+solver bit for bit too."""
 import socket
 
 import numpy as np
@@ -68,4 +71,31 @@ def test_rows_round_trip_through_host_and_device_memory(pkg, precision):
     T = h.get_state(4)
     assert np.array_equal(T[0:2], S[20:22]) and np.array_equal(T[10:13], S[5:8])
     assert np.array_equal(T[2:10], S[2:10]) and np.array_equal(T[13:], S[13:])
+    h.close()
+
+
+NCCL_CASES = [dict(world=1, nx=96, ny=80, seed=3, strategy=s, width=1.0, height=0.9, t_end=0.05, precision=p, first=7)
+              for s, p in [(0, 0), (5, 0), (4, 3), (2, 1)]]
+
+
+@pytest.mark.parametrize("case", NCCL_CASES, ids=lambda c: f"strategy{c['strategy']}-prec{c['precision']}")
+def test_device_enqueued_slab_steps_over_nccl_equal_single_solver(pkg, case, tmp_path):
+    out = str(tmp_path / "gathered.npz")
+    mp.spawn(slab_ranks.nccl_worker, args=(case["world"], free_port(), case, out), nprocs=case["world"], join=True)
+    z = np.load(out)
+    G, t, steps = z["G"], float(z["t"]), int(z["steps"])
+    assert int(z["first"]) == case["first"]
+    V, vt, vsteps = single(pkg, case)
+    assert (steps, t) == (vsteps, vt)
+    assert np.array_equal(G, V, equal_nan=True)
+
+
+def test_async_row_transfers_refuse_host_memory(pkg):
+    nx, ny = 40, 30
+    h = pkg.Handle(nx, ny)
+    h.configure(1.0, 1.0, 0.1, 0.45, 1.9, 1.4, 0, 0)
+    h.set_state(pkg.scenarios.seeded_four_quadrant(nx, ny, 1))
+    host = np.zeros((4, 2, nx))
+    with pytest.raises(pkg.FVM2DError):
+        h.get_rows_async(0, 2, host.ctypes.data)
     h.close()
