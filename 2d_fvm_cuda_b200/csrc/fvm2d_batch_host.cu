@@ -93,6 +93,11 @@ struct fvm2d_batch {
     int *rb0_d = nullptr, *ib0_d = nullptr;
     BatchLaunch L{};
     bool dirty = true;  // descriptors must be rebuilt and uploaded
+    // problems whose sweep items are in the item lists: all at the start of a
+    // run; problems whose loop has ended are dropped from the lists (and the
+    // step graphs re-captured) once they hold a sizeable share of the items,
+    // so the static split of items over warps keeps every warp on live work
+    std::vector<char> listed;
     int T = 32;         // y-sweep interfaces per segment
     int grid_x = 0, grid_y = 0;
     int occ_x = 1, occ_y = 1;
@@ -118,8 +123,8 @@ struct fvm2d_batch {
     {
         if (!dirty) return FVM2D_OK;
         std::vector<BatchProblem> P(np);
-        std::vector<long long> x0(np + 1, 0), y0(np + 1, 0);
         std::vector<int> rb0(np + 1, 0), ib0(np + 1, 0);
+        if ((int)listed.size() != np) listed.assign(np, 1);
         // offsets in elements of the storage type: FP32 planes start at the
         // same byte addresses as FP64 planes would (the layout is in doubles)
         const long long scale = (precision == FVM2D_FP32) ? 2 : 1;
@@ -144,23 +149,19 @@ struct fvm2d_batch {
             q.plan.cfl = cfl[p];
             q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
             q.plan.fixed_dt = 0.0;
-            q.nsegx = (nx[p] - 4 + 29) / 30;
+            q.nsegx = fvm2d::x_items_per_row(nx[p]);
             q.ncw = (nx[p] + 31) / 32;
             q.T = T;
             q.nsegy = y_segments(ny[p], T);
             q.ring = 4 * nx[p] + 4 * (ny[p] - 4);
-            x0[p + 1] = x0[p] + (long long)q.nsegx * ny[p];
-            y0[p + 1] = y0[p] + (long long)q.ncw * q.nsegy;
             rb0[p + 1] = rb0[p] + (q.ring + kGhostThreads - 1) / kGhostThreads;
             const long long cells = (long long)nx[p] * ny[p];
             ib0[p + 1] = ib0[p] + int((cells + fvm2d::kBatchInitCells - 1) / fvm2d::kBatchInitCells);
         }
         CK(cudaMemcpyAsync(prob_d, P.data(), sizeof(BatchProblem) * np, cudaMemcpyHostToDevice, stream));
-        CK(cudaMemcpyAsync(x0_d, x0.data(), sizeof(long long) * (np + 1), cudaMemcpyHostToDevice, stream));
-        CK(cudaMemcpyAsync(y0_d, y0.data(), sizeof(long long) * (np + 1), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(rb0_d, rb0.data(), sizeof(int) * (np + 1), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(ib0_d, ib0.data(), sizeof(int) * (np + 1), cudaMemcpyHostToDevice, stream));
-        CK(cudaStreamSynchronize(stream));
+        if (int rc = upload_items()) return rc;
         L.base = base;
         L.prob = prob_d;
         L.ctl = ctl_d;
@@ -169,8 +170,6 @@ struct fvm2d_batch {
         L.rb0 = rb0_d;
         L.ib0 = ib0_d;
         L.np = np;
-        L.x_total = x0[np];
-        L.y_total = y0[np];
         L.ring_blocks = rb0[np];
         L.init_blocks = ib0[np];
         L.grid_x = grid_x;
@@ -178,6 +177,41 @@ struct fvm2d_batch {
         dirty = false;
         drop_graphs();
         return FVM2D_OK;
+    }
+
+    // Sweep items of one row or column group of problem p.
+    long long x_items(int p) const { return (long long)fvm2d::x_items_per_row(nx[p]) * ny[p]; }
+    long long y_items(int p) const { return (long long)((nx[p] + 31) / 32) * y_segments(ny[p], T); }
+
+    // Item prefix counts of the listed problems (others get no items) -> device.
+    int upload_items()
+    {
+        std::vector<long long> x0(np + 1, 0), y0(np + 1, 0);
+        for (int p = 0; p < np; ++p) {
+            x0[p + 1] = x0[p] + (listed[p] ? x_items(p) : 0);
+            y0[p + 1] = y0[p] + (listed[p] ? y_items(p) : 0);
+        }
+        CK(cudaMemcpyAsync(x0_d, x0.data(), sizeof(long long) * (np + 1), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(y0_d, y0.data(), sizeof(long long) * (np + 1), cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        L.x_total = x0[np];
+        L.y_total = y0[np];
+        return FVM2D_OK;
+    }
+
+    // After a graph replay: drops the problems whose loop has ended from the
+    // item lists once they hold at least a quarter of the listed x items.
+    int compact_items()
+    {
+        long long ended = 0;
+        for (int p = 0; p < np; ++p)
+            if (listed[p] && !ctl_h[p].active) ended += x_items(p);
+        if (ended == 0 || 4 * ended < L.x_total) return FVM2D_OK;
+        for (int p = 0; p < np; ++p)
+            if (!ctl_h[p].active) listed[p] = 0;
+        if (int rc = upload_items()) return rc;
+        drop_graphs();
+        return build_graphs();
     }
 
     int build_graphs()
@@ -212,6 +246,11 @@ struct fvm2d_batch {
     int run(int limit)
     {
         if (int rc = upload_descriptors()) return rc;
+        if (std::count(listed.begin(), listed.end(), 0)) {  // every problem's items back in the lists
+            listed.assign(np, 1);
+            if (int rc = upload_items()) return rc;
+            drop_graphs();
+        }
         if (int rc = build_graphs()) return rc;
         std::vector<int> before(np);
         for (int p = 0; p < np; ++p) {
@@ -234,6 +273,7 @@ struct fvm2d_batch {
             bool any = false;
             for (int p = 0; p < np && !any; ++p) any = ctl_h[p].active != 0;
             if (!any) break;
+            if (int rc = compact_items()) return rc;
         }
         CK(cudaEventRecord(ev1, stream));
         CK(cudaEventSynchronize(ev1));

@@ -51,6 +51,18 @@ struct LaunchConfig {
 // Kernels per step: sweep X, sweep Y, sweep Y, sweep X + average, ghost ring.
 constexpr int kStepKernels = 5;
 
+// x-sweep work items: a warp walks kXItemChunks chunks of 32 cells of one row
+// and updates kXItemCells cells (the first chunk's first two lanes only feed
+// their neighbours).  Item seg of a row updates cells 2 + kXItemCells seg ..
+// 1 + kXItemCells (seg + 1); a row of nx cells has
+// (nx - 4 + kXItemCells - 1) / kXItemCells items.
+#ifndef FVM2D_X_CHUNKS
+#define FVM2D_X_CHUNKS 4
+#endif
+constexpr int kXItemChunks = FVM2D_X_CHUNKS;
+constexpr int kXItemCells = 32 * kXItemChunks - 2;
+__host__ __device__ constexpr int x_items_per_row(int nx) { return (nx - 4 + kXItemCells - 1) / kXItemCells; }
+
 // The entry points each build of the kernels provides (namespaces fp64,
 // fp64_strict, fp64_reforder, fp32, and jvp: FP64 values with tangents).
 #define FVM2D_DECLARE_VARIANT(ns)                                              \

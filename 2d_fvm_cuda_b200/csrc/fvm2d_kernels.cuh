@@ -275,12 +275,9 @@ __device__ __forceinline__ Cell<Real> shfl_last(const Cell<Real> &c)
 
 // Chunks of 32 cells per x-sweep work item, and the cells an item updates:
 // item seg starts at cell b0 = 1 + kXCells seg (lane 0 of its first chunk)
-// and updates cells b0+1 .. b0+kXCells.
-#ifndef FVM2D_X_CHUNKS
-#define FVM2D_X_CHUNKS 4
-#endif
-constexpr int kXChunks = FVM2D_X_CHUNKS;
-constexpr int kXCells = 32 * kXChunks - 2;
+// and updates cells b0+1 .. b0+kXCells (fvm2d_control.h).
+constexpr int kXChunks = kXItemChunks;
+constexpr int kXCells = kXItemCells;
 
 // One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
 // wave speed of the interior cells written by a final sweep, and bad whether

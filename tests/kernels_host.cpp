@@ -280,7 +280,7 @@ int kh_batch_solve(int np, const int *nx, const int *ny, const double *params, c
         q.plan.cfl = pr[3];
         q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
         q.plan.fixed_dt = 0.0;
-        q.nsegx = (nx[p] - 4 + 29) / 30;
+        q.nsegx = fvm2d::x_items_per_row(nx[p]);
         q.ncw = (nx[p] + 31) / 32;
         q.T = T;
         q.nsegy = y_segments(ny[p], T);

@@ -33,6 +33,8 @@ template <typename T>
 static inline T __shfl_down_sync(unsigned, T v, int) { return v; }
 template <typename T>
 static inline T __shfl_up_sync(unsigned, T v, int) { return v; }
+template <typename T>
+static inline T __shfl_sync(unsigned, T v, int) { return v; }
 
 #define FVM2D_VARIANT host
 #define FVM2D_REAL double
