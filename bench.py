@@ -304,6 +304,15 @@ def product_arm(args, rank, world, local_rank):
                     fp32_configs[key] = fn(args, with_reference_order=False)
                 except Exception as e:  # noqa: BLE001
                     fp32_configs[key] = {"error": f"{type(e).__name__}: {e}"}
+        # the batched form on its workload (256 uneven four-quadrant problems),
+        # FP64, against the same problems solved one at a time
+        batch = None
+        if world == 1 and not args.no_configs:
+            try:
+                batch = _batch_case(pkg, pkg.scenarios.uneven_batch(256, 3), ((pkg.FP64, "fp64"),),
+                                    "256 problems, sides 128..1024")[0]
+            except Exception as e:  # noqa: BLE001
+                batch = {"error": f"{type(e).__name__}: {e}"}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
@@ -333,6 +342,7 @@ def product_arm(args, rank, world, local_rank):
             "reference_cuda": ref_cuda,
             "fp32": fp32,
             "fp32_configs": fp32_configs,
+            "batch": batch,
             "adjoint": adjoint,
             "clocks": clocks,
             "gpu_launches": launches,

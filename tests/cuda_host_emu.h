@@ -147,6 +147,7 @@ static inline T __shfl_sync(unsigned, T v, int src)
     return emu::exchange(v, (src & (emu::kLanes - 1)) - emu::flat_thread() % emu::kLanes);
 }
 static inline void __syncthreads() { emu::block_bar.wait(); }
+static inline void __syncwarp(unsigned = 0xffffffffu) { emu::warp_bar[emu::flat_thread() / emu::kLanes].wait(); }
 static inline void __threadfence() {}
 static inline int __any_sync(unsigned, int p) { return emu::vote_any(p); }
 static inline long long __double_as_longlong(double x)

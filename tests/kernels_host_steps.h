@@ -137,8 +137,7 @@ void transpose(int dir, Planes<A> &U, Planes<A> &F, Planes<A> &ub, Planes<A> &ou
     if (dir == 0)
         emu::launch(dim3(1), dim3(ANT), true, [&] { adjoint_x_kernel(g); });
     else
-        emu::launch(dim3((U.nx + kTileCols - 1) / kTileCols, (U.ny + kLineOut - 1) / kLineOut), dim3(ANT), true,
-                    [&] { adjoint_y_kernel(g); });
+        emu::launch(adjoint_y_grid(U.nx, U.ny), dim3(ANT), true, [&] { adjoint_y_kernel(g); });
 }
 
 

@@ -113,9 +113,16 @@ def cpu_worker(rank, world, port, case, out_path):
 
         orc = Oracle(threads=1)
         U = initial_state(case["nx"], case["ny"], case["seed"], case["strategy"])
-        S = pkg.slab.SlabSolver(U, width=case["width"], height=case["height"], t_end=case["t_end"],
-                                cfl=0.45, alpha=1.9, gamma=1.4, strategy=case["strategy"],
-                                make_local=lambda nx, rows: OracleSlab(orc, nx, rows))
+        kw = dict(width=case["width"], height=case["height"], t_end=case["t_end"], cfl=0.45, alpha=1.9, gamma=1.4,
+                  strategy=case["strategy"], make_local=lambda nx, rows: OracleSlab(orc, nx, rows))
+        if case.get("rows_fn"):
+            # the state given as a function of the global rows; a few steps,
+            # then this rank's rows loaded again and the run restarted
+            S = pkg.slab.SlabSolver(lambda lo, hi: U[lo:hi], shape=U.shape[:2], **kw)
+            S.advance(3)
+            S.set_local_state(U[S.l_lo:S.l_hi])
+        else:
+            S = pkg.slab.SlabSolver(U, **kw)
         S.advance(case["steps"])
         G = S.gather()
         if rank == 0:  # through a file: a pipe would block on results above its 64 KB buffer

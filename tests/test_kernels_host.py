@@ -309,14 +309,15 @@ def adjoint_case(oracle, pkg, strategy, nx=37, ny=29, width=1.0, height=0.8):
     return U, dt, rng
 
 
-@pytest.mark.parametrize("strategy", range(7))
-def test_adjoint_kernels_transpose_the_forward_items(kh, oracle, pkg, strategy):
+@pytest.mark.parametrize("strategy,nx,ny", [(s, 37, 29) for s in range(7)] + [(0, 300, 263), (5, 259, 301)])
+def test_adjoint_kernels_transpose_the_forward_items(kh, oracle, pkg, strategy, nx, ny):
     """One step: the tangent J v from the forward items on dual numbers and
     the cotangent J^T w from the adjoint kernels satisfy <J v, w> =
     <v, J^T w> to rounding; the dual run's values are the step itself
-    (checked against the oracle)."""
-    nx, ny, width, height, t = 37, 29, 1.0, 0.8, 0.01
-    U, dt, rng = adjoint_case(oracle, pkg, strategy)
+    (checked against the oracle).  The larger arrays take several walk items
+    per line, each of several chunks."""
+    width, height, t = 1.0, 0.8, 0.01
+    U, dt, rng = adjoint_case(oracle, pkg, strategy, nx, ny)
     v = np.ascontiguousarray(rng.standard_normal(U.shape))
     w = np.ascontiguousarray(rng.standard_normal(U.shape))
     out, Jv, JTw = np.empty_like(U), np.empty_like(U), np.empty_like(U)

@@ -60,10 +60,13 @@ CASES = [
     dict(world=2, nx=48, ny=42, seed=7, strategy=1, width=1.0, height=1.0, t_end=0.02, steps=10),
     dict(world=3, nx=40, ny=50, seed=8, strategy=2, width=1.0, height=1.0, t_end=0.001, steps=10),
     dict(world=2, nx=40, ny=44, seed=9, strategy=3, width=1.0, height=1.0, t_end=0.001, steps=10),
+    # the state given as a function of the rows, and a restart from it
+    dict(world=3, nx=36, ny=47, seed=11, strategy=0, width=1.0, height=1.0, t_end=0.05, steps=9, rows_fn=True),
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=lambda c: f"world{c['world']}-strategy{c['strategy']}")
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"world{c['world']}-strategy{c['strategy']}"
+                         + ("-rows_fn" if c.get("rows_fn") else ""))
 def test_slab_run_equals_single_array_run(oracle, case, tmp_path):
     out = str(tmp_path / "gathered.npz")
     mp.spawn(slab_ranks.cpu_worker, args=(case["world"], free_port(), case, out), nprocs=case["world"], join=True)
