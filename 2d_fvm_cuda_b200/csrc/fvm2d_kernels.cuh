@@ -273,110 +273,8 @@ __device__ __forceinline__ Cell<Real> shfl_last(const Cell<Real> &c)
     return o;
 }
 
-// Chunks of 32 cells per x-sweep work item, and the cells an item updates:
-// item seg starts at cell b0 = 1 + kXCells seg (lane 0 of its first chunk)
-// and updates cells b0+1 .. b0+kXCells (fvm2d_control.h).
-constexpr int kXChunks = kXItemChunks;
-constexpr int kXCells = kXItemCells;
-
-// One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
-// wave speed of the interior cells written by a final sweep, and bad whether
-// one of them holds NaN or a non-positive density or pressure; a TAPE sweep
-// also stores every interface flux it computes.
-template <typename Real, class Phys, bool FINAL, bool TAPE = false>
-__device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int y, int seg,
-                                       int nseg, int lane, double &vmax, int &bad)
-{
-    const int nx = a.nx, ny = a.ny;
-    const int b0 = 1 + seg * kXCells;
-    const int last = min(b0 + kXCells, nx - 3);  // last cell this item updates
-    auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
-    auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
-        if (FINAL) {
-            Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
-            o.rho = (Ab.rho + U.rho) * Real(0.5);
-            o.p = (Ab.p + U.p) * Real(0.5);
-            o.un = (Ab.un + U.un) * Real(0.5);
-            o.ut = (Ab.ut + U.ut) * Real(0.5);
-            store_cell(a.dst, x, y, 2, 3, o);
-            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3) {
-                vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
-                bad |= !(o.rho > Real(0) && o.p > Real(0));  // NaN fails both tests
-            }
-        } else {
-            store_cell(a.dst, x, y, 2, 3, U);
-        }
-    };
-    Cell<Real> cs = {Real(0), Real(0), Real(0), Real(0)}, cF = cs;  // lane 31's slope and flux, previous chunk
-    for (int j = 0; j < kXChunks; ++j) {
-        const int b = b0 + 32 * j;
-        if (b - 1 > last) break;  // nothing left to update (the same for the whole warp)
-        const int c = b + lane, u = c - 1;  // this lane's cell, and the cell it updates
-        const Cell<Real> cm1 = ld(c - 1), c0 = ld(c), cp1 = ld(c + 1);
-        Cell<Real> A;
-        if (FINAL) A = load_cell(a.comb, min(max(u, 0), nx - 1), y, 2, 3);  // branch A, loaded early
-        const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);                // slope of cell c
-        Cell<Real> sm1 = shfl_up(s0);                                     // slope of cell c-1
-        if (lane == 0) sm1 = cs;
-        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
-        if (c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);   // interface c-1/2
-        if (TAPE && (j > 0 || lane >= 1) && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // at cell c
-        Cell<Real> FL = shfl_up(F);                                       // interface c-3/2
-        if (lane == 0) FL = cF;
-        if ((j > 0 || lane >= 2) && u <= last) emit(u, Phys::update(cm1, FL, F, K), A);
-        cs = shfl_last(s0);
-        cF = shfl_last(F);
-    }
-    // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
-    if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
-        const int x = seg == 0 ? lane : nx - 2 + lane;
-        Cell<Real> Ab;
-        if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
-        emit(x, ld(x), Ab);
-        if (seg == 0 && seg == nseg - 1) {
-            const int x2 = nx - 2 + lane;
-            if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
-            emit(x2, ld(x2), Ab);
-        }
-    }
-}
-
-template <typename Real, class Phys, bool FINAL, int NT, int MINB, bool TAPE = false>
-__global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
-{
-    if (!a.ctl->active) return;
-    const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
-    const int lane = threadIdx.x & 31;
-    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
-    const long long nwork = (long long)nseg * a.ny;
-    const long long wstride = (long long)gridDim.x * (NT / 32);
-    double vmax = 0.0;
-    int bad = 0;
-    for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
-        x_item<Real, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax, bad);
-    if (FINAL) {
-        note_bad_cells(bad, a.ctl);
-        block_max_to<NT>(vmax, &a.ctl->smax_bits);
-    }
-}
-
-// Segments of T interfaces (T-1 updated cells) along a y line of ny cells.
-__host__ __device__ __forceinline__ int y_segments(int ny, int T) { return (ny - 4 + T - 2) / (T - 1); }
-
-// One y-sweep work item: columns 32 cw .. 32 cw + 31, segment seg (of nseg)
-// of T interfaces.  A TAPE sweep also stores every interface flux.
-//
-// RING = 0: the walker keeps its three cells, the next one (loaded one
-// interface ahead), the last slope and the last flux in registers.
-// RING = D > 0: each lane streams its column through a ring of kYRingRows
-// rows in shared memory (`ring`, rows of 4 fields, consecutive entries
-// `rs` elements apart, one column per thread), filled by asynchronous
-// global->shared copies issued D rows ahead of use and waited for per
-// thread (cp.async groups: no barrier, no other thread involved); the
-// registers then hold only the last slope and flux across the Riemann
-// solver, and the loads never stall the walker.
-constexpr int kYRingRows = 8;
-
+// Asynchronous global->shared copies of single elements (cp.async groups,
+// waited for by the issuing thread).
 template <typename Real>
 __device__ __forceinline__ void async_copy(Real *dst_shared, const Real *src)
 {
@@ -403,6 +301,173 @@ __device__ __forceinline__ void async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 #endif
 }
+
+// Chunks of 32 cells per x-sweep work item, and the cells an item updates:
+// item seg starts at cell b0 = 1 + kXCells seg (lane 0 of its first chunk)
+// and updates cells b0+1 .. b0+kXCells (fvm2d_control.h).
+constexpr int kXChunks = kXItemChunks;
+constexpr int kXCells = kXItemCells;
+
+// One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
+// wave speed of the interior cells written by a final sweep, and bad whether
+// one of them holds NaN or a non-positive density or pressure; a TAPE sweep
+// also stores every interface flux it computes.
+//
+// RING = D > 0: the warp streams its row through a ring of kXRingChunks
+// chunk slots in shared memory (`ring`: this warp's slots, 4 fields of 32
+// cells each), filled by asynchronous copies D chunks ahead of use; a lane
+// reads its three cells there instead of from global memory.
+constexpr int kXRingChunks = 8;
+#ifndef FVM2D_X_RING
+#define FVM2D_X_RING 0
+#endif
+
+template <typename Real, class Phys, bool FINAL, bool TAPE = false, int RING = 0>
+__device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int y, int seg,
+                                       int nseg, int lane, double &vmax, int &bad, Real *ring = nullptr)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int b0 = 1 + seg * kXCells;
+    const int last = min(b0 + kXCells, nx - 3);  // last cell this item updates
+    auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
+    auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
+        if (FINAL) {
+            Cell<Real> o;  // primitive average with branch A (src/basicFuns.cuh:264-274)
+            o.rho = (Ab.rho + U.rho) * Real(0.5);
+            o.p = (Ab.p + U.p) * Real(0.5);
+            o.un = (Ab.un + U.un) * Real(0.5);
+            o.ut = (Ab.ut + U.ut) * Real(0.5);
+            store_cell(a.dst, x, y, 2, 3, o);
+            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3) {
+                vmax = fmax(vmax, wave_speed(o.rho, o.p, o.un, o.ut, a.gamma));
+                bad |= !(o.rho > Real(0) && o.p > Real(0));  // NaN fails both tests
+            }
+        } else {
+            store_cell(a.dst, x, y, 2, 3, U);
+        }
+    };
+    // chunk m's cell of this lane into its ring slot
+    auto issue = [&](int m) {
+        const int x = min(max(b0 + 32 * m + lane, 0), nx - 1);
+        Real *r = ring + (m & (kXRingChunks - 1)) * 128 + lane;
+        async_copy(r, &a.src.at(0, x, y));
+        async_copy(r + 32, &a.src.at(1, x, y));
+        async_copy(r + 64, &a.src.at(2, x, y));
+        async_copy(r + 96, &a.src.at(3, x, y));
+    };
+    auto get = [&](int m, int k) {
+        const Real *r = ring + (m & (kXRingChunks - 1)) * 128 + k;
+        Cell<Real> q;
+        q.rho = r[0];
+        q.p = r[32];
+        q.un = r[64];
+        q.ut = r[96];
+        return q;
+    };
+    if constexpr (RING > 0) {
+        static_assert(RING + 3 <= kXRingChunks, "prefetch distance does not fit the ring");
+        issue(0);
+        issue(1);
+        async_commit();
+        for (int m = 2; m <= RING; ++m) {
+            issue(m);
+            async_commit();
+        }
+    }
+    Cell<Real> cs = {Real(0), Real(0), Real(0), Real(0)}, cF = cs;  // lane 31's slope and flux, previous chunk
+    for (int j = 0; j < kXChunks; ++j) {
+        const int b = b0 + 32 * j;
+        if (b - 1 > last) break;  // nothing left to update (the same for the whole warp)
+        const int c = b + lane, u = c - 1;  // this lane's cell, and the cell it updates
+        Cell<Real> cm1, c0, cp1;
+        if constexpr (RING > 0) {
+            issue(j + RING + 1);
+            async_commit();
+            async_wait<RING>();  // chunks up to j+1 have landed (this lane's copies)
+            __syncwarp();        // ... and every lane's
+            cm1 = lane > 0 ? get(j, lane - 1) : (j > 0 ? get(j - 1, 31) : ld(c - 1));
+            c0 = get(j, lane);
+            cp1 = lane < 31 ? get(j, lane + 1) : get(j + 1, 0);
+        } else {
+            cm1 = ld(c - 1);
+            c0 = ld(c);
+            cp1 = ld(c + 1);
+        }
+        Cell<Real> A;
+        if (FINAL) A = load_cell(a.comb, min(max(u, 0), nx - 1), y, 2, 3);  // branch A, loaded early
+        const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);                // slope of cell c
+        Cell<Real> sm1 = shfl_up(s0);                                     // slope of cell c-1
+        if (lane == 0) sm1 = cs;
+        Cell<Real> F = {Real(0), Real(0), Real(0), Real(0)};
+        if (c <= nx - 2) F = Phys::interface_flux(cm1, c0, sm1, s0, K);   // interface c-1/2
+        if (TAPE && (j > 0 || lane >= 1) && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // at cell c
+        Cell<Real> FL = shfl_up(F);                                       // interface c-3/2
+        if (lane == 0) FL = cF;
+        if ((j > 0 || lane >= 2) && u <= last) emit(u, Phys::update(cm1, FL, F, K), A);
+        cs = shfl_last(s0);
+        cF = shfl_last(F);
+    }
+    if constexpr (RING > 0) {
+        async_wait<0>();  // no copy of this item may land in the ring after it
+        __syncwarp();
+    }
+    // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
+    if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
+        const int x = seg == 0 ? lane : nx - 2 + lane;
+        Cell<Real> Ab;
+        if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
+        emit(x, ld(x), Ab);
+        if (seg == 0 && seg == nseg - 1) {
+            const int x2 = nx - 2 + lane;
+            if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
+            emit(x2, ld(x2), Ab);
+        }
+    }
+}
+
+template <typename Real, class Phys, bool FINAL, int NT, int MINB, bool TAPE = false>
+__global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
+{
+    if (!a.ctl->active) return;
+    const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
+    const int lane = threadIdx.x & 31;
+    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
+    const long long nwork = (long long)nseg * a.ny;
+    const long long wstride = (long long)gridDim.x * (NT / 32);
+    double vmax = 0.0;
+    int bad = 0;
+    constexpr int RING = (sizeof(Real) == 4 || sizeof(Real) == 8) ? FVM2D_X_RING : 0;
+    if constexpr (RING > 0) {
+        __shared__ Real ring[(NT / 32) * kXRingChunks * 128];
+        Real *mine = ring + (threadIdx.x / 32) * kXRingChunks * 128;
+        for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+            x_item<Real, Phys, FINAL, TAPE, RING>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax, bad, mine);
+    } else {
+        for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+            x_item<Real, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, lane, vmax, bad);
+    }
+    if (FINAL) {
+        note_bad_cells(bad, a.ctl);
+        block_max_to<NT>(vmax, &a.ctl->smax_bits);
+    }
+}
+
+// Segments of T interfaces (T-1 updated cells) along a y line of ny cells.
+__host__ __device__ __forceinline__ int y_segments(int ny, int T) { return (ny - 4 + T - 2) / (T - 1); }
+
+// One y-sweep work item: columns 32 cw .. 32 cw + 31, segment seg (of nseg)
+// of T interfaces.  A TAPE sweep also stores every interface flux.
+//
+// RING = 0: the walker keeps its three cells, the next one (loaded one
+// interface ahead), the last slope and the last flux in registers.
+// RING = D > 0: each lane streams its column through a ring of kYRingRows
+// rows in shared memory (`ring`, rows of 4 fields, consecutive entries
+// `rs` elements apart, one column per thread), filled by asynchronous
+// global->shared copies issued D rows ahead of use and waited for per
+// thread (cp.async groups: no barrier, no other thread involved); the
+// registers then hold only the last slope and flux across the Riemann
+// solver, and the loads never stall the walker.
+constexpr int kYRingRows = 8;
 
 template <typename Real, class Phys, bool TAPE = false, int RING = 0>
 __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int seg, int nseg,

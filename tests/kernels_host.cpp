@@ -138,7 +138,12 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
             int bad = 0;
             for (long long w = 0; w < nwork; ++w) {
                 const int y = int(w / nseg), seg = int(w % nseg);
-                if (policy == 0 && final)
+                static double xring[kXRingChunks * 128];  // one warp's ring
+                if (policy == 3 && final)
+                    x_item<double, RefOrder, true, false, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
+                else if (policy == 3)
+                    x_item<double, RefOrder, false, false, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
+                else if (policy == 0 && final)
                     x_item<double, RefOrder, true>(a, K, y, seg, nseg, lane, vmax, bad);
                 else if (policy == 0)
                     x_item<double, RefOrder, false>(a, K, y, seg, nseg, lane, vmax, bad);

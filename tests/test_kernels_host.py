@@ -104,7 +104,7 @@ def kh_fast(tmp_path_factory):
     return _kernels_host(tmp_path_factory, ("FVM2D_FAST_RCP",))
 
 
-REF, HOISTED, REF_RING = 0, 1, 2
+REF, HOISTED, REF_RING, REF_XRING = 0, 1, 2, 3
 ALPHA, GAMMA = 1.9, 1.4
 
 
@@ -120,7 +120,7 @@ def sweep(kh, policy, direction, U, h, dt, T=16, comb=None):
     return out
 
 
-SWEEP_SIZES = [(48, 32), (37, 29), (33, 7), (6, 6), (70, 12)]
+SWEEP_SIZES = [(48, 32), (37, 29), (33, 7), (6, 6), (70, 12), (300, 9)]
 
 
 def ghost(kh, U, strategy, t, row0=0, gny=None, top=True, bottom=True, gamma=1.4):
@@ -151,6 +151,8 @@ def test_sweep_items_equal_the_oracle_sweeps(kh, oracle, pkg, nx, ny):
     U, width, height, dt = sweep_case(pkg, oracle, nx, ny, 3)
     X = sweep(kh, REF, 0, U, width / nx, dt)
     assert np.array_equal(X, oracle.sweep_x(U, width, dt))  # every cell written, bit for bit
+    # the x walker that streams its row through the shared-memory ring
+    assert np.array_equal(sweep(kh, REF_XRING, 0, U, width / nx, dt), X)
     RY = oracle.sweep_y(U, height, dt)
     for T in (8, 16, 32, 64, 4):  # the kernels choose 64, 32, 16 or 8; 4 for short segments
         assert np.array_equal(sweep(kh, REF, 1, U, height / ny, dt, T), RY), T
