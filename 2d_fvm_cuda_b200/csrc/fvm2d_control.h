@@ -57,7 +57,7 @@ constexpr int kStepKernels = 5;
 // 1 + kXItemCells (seg + 1); a row of nx cells has
 // (nx - 4 + kXItemCells - 1) / kXItemCells items.
 #ifndef FVM2D_X_CHUNKS
-#define FVM2D_X_CHUNKS 4
+#define FVM2D_X_CHUNKS 8
 #endif
 constexpr int kXItemChunks = FVM2D_X_CHUNKS;
 constexpr int kXItemCells = 32 * kXItemChunks - 2;

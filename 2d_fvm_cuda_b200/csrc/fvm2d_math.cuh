@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 #ifndef FVM2D_VARIANT
 #error "define FVM2D_VARIANT (the namespace of this build of the kernels) first"
@@ -50,10 +51,26 @@ __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 // within a couple of ulp of correctly rounded ones (not bit-identical: that
 // build is held to the reference within a relative L1 tolerance).  Each costs
 // the seed and three to five FP64 operations instead of a full IEEE division
-// or square-root sequence.  Other builds use IEEE division and CUDA's rsqrt
+// or square-root sequence.  The seeds flush subnormal arguments to zero and
+// the refinement needs a finite, normal seed, so arguments of magnitude
+// outside [2^-999, 2^999) (zero, subnormal, huge, infinite, NaN: only ever
+// met in near-vacuum, degenerate or corrupt states) take IEEE division and
+// CUDA's rsqrt instead.  Other builds use IEEE division and CUDA's rsqrt
 // (1 ulp); rsqrtf is within 2 ulp; the dual-number overloads live with the
 // dual type, and other number types divide.
 #if defined(FVM2D_FAST_RCP)
+// 2^-999 <= |x| < 2^999, from the biased exponent of x
+__device__ __forceinline__ bool seed_range(double x)
+{
+#if defined(__CUDA_ARCH__)
+    const unsigned hi = unsigned(__double2hiint(x));
+#else
+    unsigned long long bits;
+    memcpy(&bits, &x, sizeof bits);
+    const unsigned hi = unsigned(bits >> 32);
+#endif
+    return ((hi >> 20) & 0x7ffu) - 24u < 1998u;
+}
 __device__ __forceinline__ double rcp_seed(double x)
 {
 #if defined(__CUDA_ARCH__)
@@ -61,7 +78,7 @@ __device__ __forceinline__ double rcp_seed(double x)
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
     return r;
 #else
-    return double(1.0f / float(x));  // host builds of this file (tests): a single-precision seed
+    return (1.0 / x) * (1.0 + 0x1p-21);  // host builds of this file (tests): a seed 2^-21 off
 #endif
 }
 __device__ __forceinline__ double rsqrt_seed(double x)
@@ -71,20 +88,32 @@ __device__ __forceinline__ double rsqrt_seed(double x)
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
     return r;
 #else
-    return double(1.0f / sqrtf(float(x)));
+    return (1.0 / sqrt(x)) * (1.0 - 0x1p-21);
 #endif
 }
 __device__ __forceinline__ double rrcp(double x)
 {
-    const double r = rcp_seed(x);
-    const double e = fma(-x, r, 1.0);
-    return fma(r, fma(e, e, e), r);
+    if (!seed_range(x)) return 1.0 / x;
+    double r = rcp_seed(x);
+    double e = fma(-x, r, 1.0);
+    r = fma(r, fma(e, e, e), r);
+#if defined(FVM2D_RCP_EXTRA)
+    e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+#endif
+    return r;
 }
 __device__ __forceinline__ double rrsqrt(double x)
 {
-    const double y = rsqrt_seed(x);
-    const double e = fma(-(x * y), y, 1.0);
-    return fma(y, e * fma(e, 0.375, 0.5), y);
+    if (!seed_range(x)) return ::rsqrt(x);
+    double y = rsqrt_seed(x);
+    double e = fma(-(x * y), y, 1.0);
+    y = fma(y, e * fma(e, 0.375, 0.5), y);
+#if defined(FVM2D_RCP_EXTRA)
+    e = fma(-(x * y), y, 1.0);
+    y = fma(0.5 * y, e, y);
+#endif
+    return y;
 }
 #else
 __device__ __forceinline__ double rrcp(double x) { return 1.0 / x; }
@@ -605,12 +634,15 @@ __device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, d
     double du = double(u), dv = double(v);
 #if defined(FVM2D_FAST_RCP)
     // sqrt(q) = q / sqrt(q) and sqrt(g p / rho) = |g p| / sqrt(g p rho):
-    // two reciprocal square roots, no division; states where g p rho is not
-    // positive (invalid ones) take the reference's expression
+    // two reciprocal square roots, no division.  A speed below 2^-499 adds
+    // nothing to the maximum, so q under 2^-998 (zero included) counts as
+    // that bound (the result stays below 2^-499, and 0 for q = 0); states
+    // where g p rho is not a positive normal number (invalid or degenerate
+    // ones) take the reference's expression
     const double q = du * du + dv * dv;
-    const double velo = q > 0.0 ? q * rrsqrt(q) : 0.0;
+    const double velo = q * rrsqrt(fmax(q, 0x1p-998));
     const double gp = g * double(p), gpr = gp * double(rho);
-    const double c = gpr > 0.0 ? fabs(gp) * rrsqrt(gpr) : sqrt(gp / double(rho));
+    const double c = (gpr >= 0x1p-998 && gpr < 0x1p998) ? fabs(gp) * rrsqrt(gpr) : sqrt(gp / double(rho));
     return velo + c;
 #else
     double velo = sqrt(du * du + dv * dv);

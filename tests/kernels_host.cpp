@@ -140,9 +140,9 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
                 const int y = int(w / nseg), seg = int(w % nseg);
                 static double xring[kXRingChunks * 128];  // one warp's ring
                 if (policy == 3 && final)
-                    x_item<double, RefOrder, true, false, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
+                    x_item<double, RefOrder, true, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
                 else if (policy == 3)
-                    x_item<double, RefOrder, false, false, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
+                    x_item<double, RefOrder, false, 4>(a, K, y, seg, nseg, lane, vmax, bad, xring);
                 else if (policy == 0 && final)
                     x_item<double, RefOrder, true>(a, K, y, seg, nseg, lane, vmax, bad);
                 else if (policy == 0)
@@ -164,7 +164,7 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
                     if (policy == 0)
                         y_item<double, RefOrder>(a, K, seg, nseg, cw, lane, T);
                     else if (policy == 2)
-                        y_item<double, RefOrder, false, 4>(a, K, seg, nseg, cw, lane, T, ring.data() + lane, 32);
+                        y_item<double, RefOrder, 4>(a, K, seg, nseg, cw, lane, T, ring.data() + lane, 32);
                     else
                         y_item<double, Hoisted>(a, K, seg, nseg, cw, lane, T);
                 }

@@ -51,7 +51,7 @@ void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double d
         double vmax = 0.0;
         int bad = 0;
         for (long long w = 0; w < nwork; ++w)
-            x_item<R, Phys, FINAL, TAPE>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
+            x_item<R, Phys, FINAL>(a, K, int(w / nseg), int(w % nseg), nseg, int(threadIdx.x), vmax, bad);
     });
 }
 
@@ -64,7 +64,7 @@ void y_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double d
     const int ncw = (a.nx + 31) / 32, nseg = y_segments(a.ny, T);
     for (int seg = 0; seg < nseg; ++seg)
         for (int cw = 0; cw < ncw; ++cw)
-            for (int lane = 0; lane < 32; ++lane) y_item<R, Phys, TAPE>(a, K, seg, nseg, cw, lane, T);
+            for (int lane = 0; lane < 32; ++lane) y_item<R, Phys>(a, K, seg, nseg, cw, lane, T);
 }
 
 // One split step U -> out of the shared-reciprocal build, in the kernels'

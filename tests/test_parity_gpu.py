@@ -137,6 +137,23 @@ def test_fma_within_tolerance_after_every_step_of_the_quadrant_workload(pkg, ora
     print(f"620 steps, largest relative L1 after any step: {worst:.3g}")
 
 
+def test_fma_within_tolerance_on_a_shock_meeting_gas_at_rest(pkg, oracle):
+    """A Mach-2 shock running into gas at rest (the shock-bubble problem,
+    reflective top and bottom walls): ahead of the waves the velocities grow
+    from exactly zero through arbitrarily small values, which the product
+    build's refined reciprocals must handle like IEEE division (the loop once
+    ended after a few steps on an infinite wave speed).  Same steps as the
+    oracle and within the relative L1 tolerance."""
+    nx, ny = 256, 128
+    U0 = pkg.scenarios.shock_bubble(nx, ny, width=2.0, height=1.0, seed=0)
+    kw = dict(width=2.0, height=1.0, cfl=0.45, alpha=1.9, gamma=1.4, t_end=0.05, strategy=6)
+    O, osteps, ot = oracle.solve(U0, **kw)
+    G, steps, t = gpu_run(pkg, U0, precision=pkg.FP64, **kw)
+    assert steps == osteps and t == pytest.approx(ot, rel=0, abs=1e-15)
+    err = rel_l1(G, O)
+    assert max(err) <= REL_L1_TOL, err
+
+
 @pytest.mark.skipif(not os.path.exists(REF_GPU_NOFMA), reason="reference CUDA build not present")
 def test_reference_cuda_nofma_equals_strict(pkg):
     U0 = pkg.scenarios.seeded_four_quadrant(96, 64, 77)
