@@ -68,6 +68,7 @@ __device__ __forceinline__ SweepArgs<Real> batch_sweep_args(const BatchArgs<Real
     a.alpha = P.alpha;
     a.gamma = P.gamma;
     a.ctl = b.ctl + p;
+    a.xchunks = P.xchunks;
     a.flux.base = nullptr;  // batches do not tape
     a.flux.plane = P.plane;
     a.flux.pitch = P.pitch;

@@ -16,7 +16,7 @@ struct BatchProblem {
     int nsegx;             // x-sweep segments per row
     int ncw, nsegy, T;     // y-sweep: 32-column groups, segments per column, interfaces per segment
     int ring;              // ghost-ring cells
-    int pad;
+    int xchunks;           // x-sweep: chunks of 32 cells per work item (fvm2d_control.h)
 };
 
 // Cells per block of the batched initial wave-speed reduction.

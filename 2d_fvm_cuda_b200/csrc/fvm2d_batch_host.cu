@@ -99,6 +99,7 @@ struct fvm2d_batch {
     // so the static split of items over warps keeps every warp on live work
     std::vector<char> listed;
     int T = 32;         // y-sweep interfaces per segment
+    int xchunks = 8;    // x-sweep chunks of 32 cells per item (set with the descriptors)
     int grid_x = 0, grid_y = 0;
     int occ_x = 1, occ_y = 1;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -124,6 +125,15 @@ struct fvm2d_batch {
         if (!dirty) return FVM2D_OK;
         std::vector<BatchProblem> P(np);
         std::vector<int> rb0(np + 1, 0), ib0(np + 1, 0);
+        // one x-item length for the batch: the longest that still gives
+        // every resident warp a couple of items over all problems
+        xchunks = 8;
+        for (;;) {
+            long long items = 0;
+            for (int p = 0; p < np; ++p) items += (long long)fvm2d::x_items_per_row(nx[p], xchunks) * ny[p];
+            if (xchunks == 1 || items >= 2ll * occ_x * 4) break;
+            xchunks /= 2;
+        }
         if ((int)listed.size() != np) listed.assign(np, 1);
         // offsets in elements of the storage type: FP32 planes start at the
         // same byte addresses as FP64 planes would (the layout is in doubles)
@@ -149,7 +159,8 @@ struct fvm2d_batch {
             q.plan.cfl = cfl[p];
             q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
             q.plan.fixed_dt = 0.0;
-            q.nsegx = fvm2d::x_items_per_row(nx[p]);
+            q.xchunks = xchunks;
+            q.nsegx = fvm2d::x_items_per_row(nx[p], xchunks);
             q.ncw = (nx[p] + 31) / 32;
             q.T = T;
             q.nsegy = y_segments(ny[p], T);
@@ -180,7 +191,7 @@ struct fvm2d_batch {
     }
 
     // Sweep items of one row or column group of problem p.
-    long long x_items(int p) const { return (long long)fvm2d::x_items_per_row(nx[p]) * ny[p]; }
+    long long x_items(int p) const { return (long long)fvm2d::x_items_per_row(nx[p], xchunks) * ny[p]; }
     long long y_items(int p) const { return (long long)((nx[p] + 31) / 32) * y_segments(ny[p], T); }
 
     // Item prefix counts of the listed problems (others get no items) -> device.

@@ -51,17 +51,23 @@ struct LaunchConfig {
 // Kernels per step: sweep X, sweep Y, sweep Y, sweep X + average, ghost ring.
 constexpr int kStepKernels = 5;
 
-// x-sweep work items: a warp walks kXItemChunks chunks of 32 cells of one row
-// and updates kXItemCells cells (the first chunk's first two lanes only feed
-// their neighbours).  Item seg of a row updates cells 2 + kXItemCells seg ..
-// 1 + kXItemCells (seg + 1); a row of nx cells has
-// (nx - 4 + kXItemCells - 1) / kXItemCells items.
-#ifndef FVM2D_X_CHUNKS
-#define FVM2D_X_CHUNKS 8
-#endif
-constexpr int kXItemChunks = FVM2D_X_CHUNKS;
-constexpr int kXItemCells = 32 * kXItemChunks - 2;
-__host__ __device__ constexpr int x_items_per_row(int nx) { return (nx - 4 + kXItemCells - 1) / kXItemCells; }
+// x-sweep work items: a warp walks `chunks` chunks of 32 cells of one row and
+// updates 32 chunks - 2 cells (the first chunk's first two lanes only feed
+// their neighbours).  Item seg of a row updates cells 2 + cells seg ..
+// 1 + cells (seg + 1).  Long items waste less; an array must still give
+// every resident warp a couple of items, so the chunk count is the largest
+// of 8, 4, 2, 1 that does (x_chunks_for).
+__host__ __device__ constexpr int x_item_cells(int chunks) { return 32 * chunks - 2; }
+__host__ __device__ constexpr int x_items_per_row(int nx, int chunks)
+{
+    return (nx - 4 + x_item_cells(chunks) - 1) / x_item_cells(chunks);
+}
+inline int x_chunks_for(long long rows, int nx, long long resident_warps)
+{
+    int c = 8;
+    while (c > 1 && rows * x_items_per_row(nx, c) < 2 * resident_warps) c /= 2;
+    return c;
+}
 
 // The entry points each build of the kernels provides (namespaces fp64,
 // fp64_strict, fp64_reforder, fp32, and jvp: FP64 values with tangents).

@@ -147,6 +147,7 @@ struct SweepArgs {
     double rh;         // 1.0 / h, as the reference computes it
     double alpha, gamma;
     StepControl *ctl;
+    int xchunks;       // x-sweeps: chunks of 32 cells per work item (fvm2d_control.h)
     Field<Real> flux;  // taped sweeps only (base null otherwise): each interface's flux (planes:
                        // mass, normal momentum, energy, tangential momentum) at the interface's right cell
 };
@@ -302,11 +303,9 @@ __device__ __forceinline__ void async_wait()
 #endif
 }
 
-// Chunks of 32 cells per x-sweep work item, and the cells an item updates:
-// item seg starts at cell b0 = 1 + kXCells seg (lane 0 of its first chunk)
-// and updates cells b0+1 .. b0+kXCells (fvm2d_control.h).
-constexpr int kXChunks = kXItemChunks;
-constexpr int kXCells = kXItemCells;
+// An x-sweep work item of a.xchunks chunks of 32 cells: item seg starts at
+// cell b0 = 1 + cells seg (lane 0 of its first chunk) and updates cells
+// b0+1 .. b0+cells, cells = 32 xchunks - 2 (fvm2d_control.h).
 
 // One x-sweep work item: row y, segment seg (of nseg).  vmax collects the
 // wave speed of the interior cells written by a final sweep, and bad whether
@@ -330,8 +329,9 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
     // a taped sweep (a.flux set) stores every interface flux; the same code
     // runs taped and untaped, so both give the same bits
     const bool tape = a.flux.base != nullptr;
-    const int b0 = 1 + seg * kXCells;
-    const int last = min(b0 + kXCells, nx - 3);  // last cell this item updates
+    const int cells = x_item_cells(a.xchunks);
+    const int b0 = 1 + seg * cells;
+    const int last = min(b0 + cells, nx - 3);  // last cell this item updates
     auto ld = [&](int x) { return load_cell(a.src, min(max(x, 0), nx - 1), y, 2, 3); };
     auto emit = [&](int x, const Cell<Real> &U, const Cell<Real> &Ab) {
         if (FINAL) {
@@ -378,7 +378,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
         }
     }
     Cell<Real> cs = {Real(0), Real(0), Real(0), Real(0)}, cF = cs;  // lane 31's slope and flux, previous chunk
-    for (int j = 0; j < kXChunks; ++j) {
+    for (int j = 0; j < a.xchunks; ++j) {
         const int b = b0 + 32 * j;
         if (b - 1 > last) break;  // nothing left to update (the same for the whole warp)
         const int c = b + lane, u = c - 1;  // this lane's cell, and the cell it updates
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     if (!a.ctl->active) return;
     const SweepConsts<Real> K = sweep_consts(a, a.ctl->dt);
     const int lane = threadIdx.x & 31;
-    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
+    const int nseg = x_items_per_row(a.nx, a.xchunks);
     const long long nwork = (long long)nseg * a.ny;
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;

@@ -97,7 +97,9 @@ __device__ __forceinline__ double rrcp(double x)
     double r = rcp_seed(x);
     double e = fma(-x, r, 1.0);
     r = fma(r, fma(e, e, e), r);
-#if defined(FVM2D_RCP_EXTRA)
+#if !defined(FVM2D_RCP_ONE_STEP)
+    // a Newton step on the refined value (Markstein's final correction):
+    // the result is then almost always the correctly rounded one
     e = fma(-x, r, 1.0);
     r = fma(r, e, r);
 #endif
@@ -109,7 +111,8 @@ __device__ __forceinline__ double rrsqrt(double x)
     double y = rsqrt_seed(x);
     double e = fma(-(x * y), y, 1.0);
     y = fma(y, e * fma(e, 0.375, 0.5), y);
-#if defined(FVM2D_RCP_EXTRA)
+#if !defined(FVM2D_RSQRT_ONE_STEP)
+    // a Newton step on the refined value
     e = fma(-(x * y), y, 1.0);
     y = fma(0.5 * y, e, y);
 #endif

@@ -28,6 +28,15 @@ using fvm2d::ad::Dual;
 
 #include "kernels_host_steps.h"
 
+// chunks of 32 cells per x-sweep item used by the functions below
+static int g_xchunks = 2;
+extern "C" int kh_set_xchunks(int c)
+{
+    if (c < 1) return 1;
+    g_xchunks = c;
+    return 0;
+}
+
 using fvm2d::PlanParams;
 using fvm2d::StepControl;
 
@@ -121,6 +130,7 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
     a.dst = Field<double>{D.data(), plane, nx};
     a.comb = a.dst;
     a.flux = Field<double>{nullptr, plane, nx};
+    a.xchunks = g_xchunks;
     a.nx = nx;
     a.ny = ny;
     a.h = h;
@@ -130,7 +140,7 @@ int kh_sweep(int policy, int dir, int final, int T, const double *in, const doub
     a.ctl = nullptr;
     const SweepConsts<double> K = sweep_consts(a, dt);
     if (dir == 0) {
-        const int nseg = (nx - 4 + kXCells - 1) / kXCells;
+        const int nseg = fvm2d::x_items_per_row(nx, a.xchunks);
         const long long nwork = (long long)nseg * ny;
         emu::launch(dim3(1), dim3(32), true, [&] {
             const int lane = int(threadIdx.x);
@@ -285,7 +295,8 @@ int kh_batch_solve(int np, const int *nx, const int *ny, const double *params, c
         q.plan.cfl = pr[3];
         q.plan.hmin = (q.hy < q.hx) ? q.hy : q.hx;
         q.plan.fixed_dt = 0.0;
-        q.nsegx = fvm2d::x_items_per_row(nx[p]);
+        q.xchunks = g_xchunks;
+        q.nsegx = fvm2d::x_items_per_row(nx[p], g_xchunks);
         q.ncw = (nx[p] + 31) / 32;
         q.T = T;
         q.nsegy = y_segments(ny[p], T);
@@ -377,6 +388,7 @@ int kh_solve(const double *cells, int nx, int ny, double width, double height, d
         a.dst = dst;
         a.comb = dst;
         a.flux = Field<double>{nullptr, plane, pitch};
+        a.xchunks = g_xchunks;
         a.nx = nx;
         a.ny = ny;
         a.h = dir == 0 ? hx : hy;

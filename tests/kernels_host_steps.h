@@ -35,6 +35,7 @@ SweepArgs<R> sweep_args(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double 
     a.alpha = alpha;
     a.gamma = gamma;
     a.ctl = nullptr;
+    a.xchunks = 2;  // two chunks of 32 cells per x item: the chunk carry is exercised
     return a;
 }
 
@@ -45,7 +46,7 @@ void x_sweep(Planes<R> &src, Planes<R> &dst, Planes<R> *flux, double h, double d
 {
     const SweepArgs<R> a = sweep_args(src, dst, flux, h, alpha, gamma);
     const SweepConsts<R> K = sweep_consts(a, dt);
-    const int nseg = (a.nx - 4 + kXCells - 1) / kXCells;
+    const int nseg = fvm2d::x_items_per_row(a.nx, a.xchunks);
     const long long nwork = (long long)nseg * a.ny;
     emu::launch(dim3(1), dim3(32), true, [&] {
         double vmax = 0.0;
@@ -134,10 +135,11 @@ void transpose(int dir, Planes<A> &U, Planes<A> &F, Planes<A> &ub, Planes<A> &ou
     g.nx = U.nx;
     g.ny = U.ny;
     g.K = adjoint_consts(h, dt, alpha, gamma);
+    g.chunks = 2;  // two chunks per walk item: the carry between chunks and between items is exercised
     if (dir == 0)
         emu::launch(dim3(1), dim3(ANT), true, [&] { adjoint_x_kernel(g); });
     else
-        emu::launch(adjoint_y_grid(U.nx, U.ny), dim3(ANT), true, [&] { adjoint_y_kernel(g); });
+        emu::launch(adjoint_y_grid(U.nx, U.ny, g.chunks), dim3(ANT), true, [&] { adjoint_y_kernel(g); });
 }
 
 

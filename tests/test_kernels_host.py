@@ -153,6 +153,14 @@ def test_sweep_items_equal_the_oracle_sweeps(kh, oracle, pkg, nx, ny):
     assert np.array_equal(X, oracle.sweep_x(U, width, dt))  # every cell written, bit for bit
     # the x walker that streams its row through the shared-memory ring
     assert np.array_equal(sweep(kh, REF_XRING, 0, U, width / nx, dt), X)
+    # x items of every length the kernels choose (chunks of 32 cells per item)
+    for chunks in (1, 4, 8):
+        assert kh.kh_set_xchunks(chunks) == 0
+        try:
+            assert np.array_equal(sweep(kh, REF, 0, U, width / nx, dt), X), chunks
+            assert np.array_equal(sweep(kh, REF_XRING, 0, U, width / nx, dt), X), chunks
+        finally:
+            kh.kh_set_xchunks(2)
     RY = oracle.sweep_y(U, height, dt)
     for T in (8, 16, 32, 64, 4):  # the kernels choose 64, 32, 16 or 8; 4 for short segments
         assert np.array_equal(sweep(kh, REF, 1, U, height / ny, dt, T), RY), T
