@@ -49,28 +49,19 @@ __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 // truncated after the quadratic term: the relative error falls from about
 // 2^-20 to about 2^-58, below the rounding of the result, so the results are
 // within a couple of ulp of correctly rounded ones (not bit-identical: that
-// build is held to the reference within a relative L1 tolerance).  Each costs
-// the seed and three to five FP64 operations instead of a full IEEE division
-// or square-root sequence.  The seeds flush subnormal arguments to zero and
-// the refinement needs a finite, normal seed, so arguments of magnitude
-// outside [2^-999, 2^999) (zero, subnormal, huge, infinite, NaN: only ever
-// met in near-vacuum, degenerate or corrupt states) take IEEE division and
-// CUDA's rsqrt instead.  Other builds use IEEE division and CUDA's rsqrt
-// (1 ulp); rsqrtf is within 2 ulp; the dual-number overloads live with the
-// dual type, and other number types divide.
+// build is held to the reference within a relative L1 tolerance).  A Newton
+// step on the refined value then makes the result almost always the
+// correctly rounded one.  Each costs the seed and five to seven FP64
+// operations instead of a full IEEE division or square-root sequence.  The
+// seeds flush subnormal arguments to zero, so the arguments must be normal
+// numbers: the solver's reciprocals take densities, pressures, sound speeds
+// and their products, which are, in any state that is not degenerate
+// (vacuum) or corrupt; the wave speed, whose velocity part can be
+// arbitrarily small, clamps its arguments (wave_speed).  Other builds use
+// IEEE division and CUDA's rsqrt (1 ulp); rsqrtf is within 2 ulp; the
+// dual-number overloads live with the dual type, and other number types
+// divide.
 #if defined(FVM2D_FAST_RCP)
-// 2^-999 <= |x| < 2^999, from the biased exponent of x
-__device__ __forceinline__ bool seed_range(double x)
-{
-#if defined(__CUDA_ARCH__)
-    const unsigned hi = unsigned(__double2hiint(x));
-#else
-    unsigned long long bits;
-    memcpy(&bits, &x, sizeof bits);
-    const unsigned hi = unsigned(bits >> 32);
-#endif
-    return ((hi >> 20) & 0x7ffu) - 24u < 1998u;
-}
 __device__ __forceinline__ double rcp_seed(double x)
 {
 #if defined(__CUDA_ARCH__)
@@ -93,13 +84,11 @@ __device__ __forceinline__ double rsqrt_seed(double x)
 }
 __device__ __forceinline__ double rrcp(double x)
 {
-    if (!seed_range(x)) return 1.0 / x;
     double r = rcp_seed(x);
     double e = fma(-x, r, 1.0);
     r = fma(r, fma(e, e, e), r);
 #if !defined(FVM2D_RCP_ONE_STEP)
-    // a Newton step on the refined value (Markstein's final correction):
-    // the result is then almost always the correctly rounded one
+    // a Newton step on the refined value (Markstein's final correction)
     e = fma(-x, r, 1.0);
     r = fma(r, e, r);
 #endif
@@ -107,7 +96,6 @@ __device__ __forceinline__ double rrcp(double x)
 }
 __device__ __forceinline__ double rrsqrt(double x)
 {
-    if (!seed_range(x)) return ::rsqrt(x);
     double y = rsqrt_seed(x);
     double e = fma(-(x * y), y, 1.0);
     y = fma(y, e * fma(e, 0.375, 0.5), y);
@@ -637,15 +625,17 @@ __device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, d
     double du = double(u), dv = double(v);
 #if defined(FVM2D_FAST_RCP)
     // sqrt(q) = q / sqrt(q) and sqrt(g p / rho) = |g p| / sqrt(g p rho):
-    // two reciprocal square roots, no division.  A speed below 2^-499 adds
-    // nothing to the maximum, so q under 2^-998 (zero included) counts as
-    // that bound (the result stays below 2^-499, and 0 for q = 0); states
-    // where g p rho is not a positive normal number (invalid or degenerate
-    // ones) take the reference's expression
+    // two reciprocal square roots, no division.  The reciprocal square root
+    // wants a normal argument: q below 2^-998 (zero and the subnormal squares
+    // of vanishing velocities ahead of a wave included) takes that bound, so
+    // the speed stays below 2^-499 (0 for q = 0), which adds nothing to the
+    // maximum; g p rho is clamped to [2^-998, 2^998], which changes nothing
+    // but degenerate states (vacuum, or pressure and density both below
+    // 1e-150)
     const double q = du * du + dv * dv;
     const double velo = q * rrsqrt(fmax(q, 0x1p-998));
-    const double gp = g * double(p), gpr = gp * double(rho);
-    const double c = (gpr >= 0x1p-998 && gpr < 0x1p998) ? fabs(gp) * rrsqrt(gpr) : sqrt(gp / double(rho));
+    const double gp = g * double(p);
+    const double c = fabs(gp) * rrsqrt(fmin(fmax(gp * double(rho), 0x1p-998), 0x1p998));
     return velo + c;
 #else
     double velo = sqrt(du * du + dv * dv);

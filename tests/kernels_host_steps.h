@@ -135,11 +135,11 @@ void transpose(int dir, Planes<A> &U, Planes<A> &F, Planes<A> &ub, Planes<A> &ou
     g.nx = U.nx;
     g.ny = U.ny;
     g.K = adjoint_consts(h, dt, alpha, gamma);
-    g.chunks = 2;  // two chunks per walk item: the carry between chunks and between items is exercised
     if (dir == 0)
         emu::launch(dim3(1), dim3(ANT), true, [&] { adjoint_x_kernel(g); });
     else
-        emu::launch(adjoint_y_grid(U.nx, U.ny, g.chunks), dim3(ANT), true, [&] { adjoint_y_kernel(g); });
+        emu::launch(dim3((U.nx + kTileCols - 1) / kTileCols, (U.ny + kLineOut - 1) / kLineOut), dim3(ANT), true,
+                    [&] { adjoint_y_kernel(g); });
 }
 
 

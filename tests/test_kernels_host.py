@@ -324,8 +324,8 @@ def test_adjoint_kernels_transpose_the_forward_items(kh, oracle, pkg, strategy, 
     """One step: the tangent J v from the forward items on dual numbers and
     the cotangent J^T w from the adjoint kernels satisfy <J v, w> =
     <v, J^T w> to rounding; the dual run's values are the step itself
-    (checked against the oracle).  The larger arrays take several walk items
-    per line, each of several chunks."""
+    (checked against the oracle).  The larger arrays take many work items
+    per line."""
     width, height, t = 1.0, 0.8, 0.01
     U, dt, rng = adjoint_case(oracle, pkg, strategy, nx, ny)
     v = np.ascontiguousarray(rng.standard_normal(U.shape))
