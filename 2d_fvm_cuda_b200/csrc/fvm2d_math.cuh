@@ -49,10 +49,11 @@ __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 // truncated after the quadratic term: the relative error falls from about
 // 2^-20 to about 2^-58, below the rounding of the result, so the results are
 // within a couple of ulp of correctly rounded ones (not bit-identical: that
-// build is held to the reference within a relative L1 tolerance).  A Newton
-// step on the refined value then makes the result almost always the
-// correctly rounded one.  Each costs the seed and five to seven FP64
-// operations instead of a full IEEE division or square-root sequence.  The
+// build is held to the reference within a relative L1 tolerance; a further
+// Newton step towards correct rounding was measured to leave its distance
+// from the oracle no smaller, 5% slower).  Each costs the seed and three to
+// five FP64 operations instead of a full IEEE division or square-root
+// sequence.  The
 // seeds flush subnormal arguments to zero, so the arguments must be normal
 // numbers: the solver's reciprocals take densities, pressures, sound speeds
 // and their products, which are, in any state that is not degenerate
@@ -84,27 +85,15 @@ __device__ __forceinline__ double rsqrt_seed(double x)
 }
 __device__ __forceinline__ double rrcp(double x)
 {
-    double r = rcp_seed(x);
-    double e = fma(-x, r, 1.0);
-    r = fma(r, fma(e, e, e), r);
-#if !defined(FVM2D_RCP_ONE_STEP)
-    // a Newton step on the refined value (Markstein's final correction)
-    e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-#endif
-    return r;
+    const double r = rcp_seed(x);
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
 }
 __device__ __forceinline__ double rrsqrt(double x)
 {
-    double y = rsqrt_seed(x);
-    double e = fma(-(x * y), y, 1.0);
-    y = fma(y, e * fma(e, 0.375, 0.5), y);
-#if !defined(FVM2D_RSQRT_ONE_STEP)
-    // a Newton step on the refined value
-    e = fma(-(x * y), y, 1.0);
-    y = fma(0.5 * y, e, y);
-#endif
-    return y;
+    const double y = rsqrt_seed(x);
+    const double e = fma(-(x * y), y, 1.0);
+    return fma(y, e * fma(e, 0.375, 0.5), y);
 }
 #else
 __device__ __forceinline__ double rrcp(double x) { return 1.0 / x; }
@@ -631,12 +620,13 @@ __device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, d
     // the speed stays below 2^-499 (0 for q = 0), which adds nothing to the
     // maximum; g p rho is clamped to [2^-998, 2^998], which changes nothing
     // but degenerate states (vacuum, or pressure and density both below
-    // 1e-150)
+    // 1e-150), and where it is negative or NaN the sound speed is NaN, as the
+    // reference's square root makes it (a NaN never wins the maximum)
     const double q = du * du + dv * dv;
     const double velo = q * rrsqrt(fmax(q, 0x1p-998));
-    const double gp = g * double(p);
-    const double c = fabs(gp) * rrsqrt(fmin(fmax(gp * double(rho), 0x1p-998), 0x1p998));
-    return velo + c;
+    const double gp = g * double(p), gpr = gp * double(rho);
+    const double c = fabs(gp) * rrsqrt(fmin(fmax(gpr, 0x1p-998), 0x1p998));
+    return velo + (gpr >= 0.0 ? c : nan(""));
 #else
     double velo = sqrt(du * du + dv * dv);
     double c = sqrt(g * double(p) / double(rho));

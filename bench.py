@@ -222,6 +222,19 @@ def product_arm(args, rank, world, local_rank):
     if os.path.exists(tp) and n == N_CELLS:
         with open(tp) as f:
             traffic = json.load(f).get(top)
+    # the FP64 pipe: the dominant kernel's FP64 flops per cell (2 per FMA,
+    # from an ncu count of its executed FP64 instructions, size-independent)
+    # over its launch time, against the device's FP64 FMA rate measured here
+    fp64_pipe = None
+    fp = os.path.join(ROOT, "profiles", "fp64_flops_per_cell.json")
+    if os.path.exists(fp) and prec == pkg.FP64:
+        with open(fp) as f:
+            per_cell = json.load(f).get(top)
+        if per_cell:
+            peak_tf, _ = pkg.measure_fp64_peak()
+            ach_tf = per_cell * n * n / (top_ms / 1e3) / 1e12
+            fp64_pipe = {"flops_per_cell": per_cell, "achieved_tflops": ach_tf, "peak_tflops": peak_tf,
+                         "peak_kind": "measured (fvm2d_measure_fp64_peak)", "frac": ach_tf / peak_tf}
 
     # L1 difference of the FMA product from the contraction-free build on the same steps
     hs = pkg.Handle(n, n)
@@ -330,7 +343,7 @@ def product_arm(args, rank, world, local_rank):
                     "path": "fvm2d_set_state(pinned) + steps x fvm2d_advance(1) + fvm2d_get_state(pinned)"},
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "alg_bytes_per_launch": alg_bytes[top], "ms_per_launch": top_ms,
+                         "alg_bytes_per_launch": alg_bytes[top], "ms_per_launch": top_ms, "fp64_pipe": fp64_pipe,
                          "share_of_step": share,
                          "kernel_ms": dict(zip(["sweep_x", "sweep_y_1", "sweep_y_2", "sweep_x_final", "ghost_fill"],
                                                kernel_ms))},
