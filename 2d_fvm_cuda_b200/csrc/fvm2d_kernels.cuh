@@ -317,8 +317,9 @@ __device__ __forceinline__ void async_wait()
 // cells each), filled by asynchronous copies D chunks ahead of use; a lane
 // reads its three cells there instead of from global memory.
 constexpr int kXRingChunks = 8;
+// prefetch distance (chunks) of the first x-sweep's ring; 0: no ring
 #ifndef FVM2D_X_RING
-#define FVM2D_X_RING 0
+#define FVM2D_X_RING 4
 #endif
 
 template <typename Real, class Phys, bool FINAL, int RING = 0>
@@ -439,7 +440,9 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
     int bad = 0;
-    constexpr int RING = (sizeof(Real) == 4 || sizeof(Real) == 8) ? FVM2D_X_RING : 0;
+    // the ring serves the first x-sweep; the final one (which also reads
+    // branch A and reduces over the block) was measured slower with it
+    constexpr int RING = (!FINAL && (sizeof(Real) == 4 || sizeof(Real) == 8)) ? FVM2D_X_RING : 0;
     if constexpr (RING > 0) {
         __shared__ Real ring[(NT / 32) * kXRingChunks * 128];
         Real *mine = ring + (threadIdx.x / 32) * kXRingChunks * 128;

@@ -622,11 +622,14 @@ __device__ __forceinline__ double wave_speed(Real rho, Real p, Real u, Real v, d
     // but degenerate states (vacuum, or pressure and density both below
     // 1e-150), and where it is negative or NaN the sound speed is NaN, as the
     // reference's square root makes it (a NaN never wins the maximum)
-    const double q = du * du + dv * dv;
-    const double velo = q * rrsqrt(fmax(q, 0x1p-998));
-    const double gp = g * double(p), gpr = gp * double(rho);
-    const double c = fabs(gp) * rrsqrt(fmin(fmax(gpr, 0x1p-998), 0x1p998));
-    return velo + (gpr >= 0.0 ? c : nan(""));
+    // (every product and sum is rounded on its own -- no contraction choice
+    // left to the compiler -- so the init, final-sweep and ghost kernels give
+    // the same bits for the same cell, and a resumed run the same dt)
+    const double q = fma(du, du, __dmul_rn(dv, dv));
+    const double velo = __dmul_rn(q, rrsqrt(fmax(q, 0x1p-998)));
+    const double gp = __dmul_rn(g, double(p)), gpr = __dmul_rn(gp, double(rho));
+    const double c = __dmul_rn(fabs(gp), rrsqrt(fmin(fmax(gpr, 0x1p-998), 0x1p998)));
+    return __dadd_rn(velo, gpr >= 0.0 ? c : nan(""));
 #else
     double velo = sqrt(du * du + dv * dv);
     double c = sqrt(g * double(p) / double(rho));

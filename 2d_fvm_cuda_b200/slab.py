@@ -303,6 +303,11 @@ class SlabSolver:
     def owned_rows(self) -> np.ndarray:
         """This rank's rows [lo, hi) of the state, shape (hi-lo, nx, 4); the
         wrapped ghost rows of a periodic run are refreshed first.  Collective."""
+        return np.ascontiguousarray(np.moveaxis(self.owned_planes(), 0, -1))
+
+    def owned_planes(self, out: np.ndarray | None = None) -> np.ndarray:
+        """As owned_rows, as planes (4, hi-lo, nx), into `out` if given (a
+        pinned buffer makes the download fast).  Collective."""
         if not self.fresh:
             if self.on_device:
                 import torch
@@ -313,8 +318,7 @@ class SlabSolver:
             else:
                 self.exchange()
             self.fresh = True
-        R = self.local.get_rows(self.lo - self.l_lo, self.hi - self.lo)
-        return np.ascontiguousarray(np.moveaxis(R, 0, -1))
+        return self.local.get_rows(self.lo - self.l_lo, self.hi - self.lo, out=out)
 
     def gather(self) -> np.ndarray | None:
         """The whole state on rank 0 (None elsewhere).  Collective."""

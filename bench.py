@@ -95,6 +95,26 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def samples(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except Exception:
+            return 0
+
+    def busy_until_sampled(self, work, more: int = 0, limit_s: float = 3.0):
+        """Runs `work` (untimed GPU steps) until `more` samples beyond the
+        current count (at least one in all) have been recorded, or limit_s."""
+        if self.proc is None:
+            work()
+            return
+        want = max(1, self.samples() + more)
+        t0 = time.perf_counter()
+        while True:
+            work()
+            if self.samples() >= want or time.perf_counter() - t0 > limit_s:
+                return
+
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -187,10 +207,13 @@ def product_arm(args, rank, world, local_rank):
 
     sampler = ClockSampler(local_rank)
     sampler.start()
-    h.advance(8)  # untimed pre-roll while the clock sampler starts
+    # untimed steps until the clock sampler has recorded under load (the
+    # timed region lasts tens of milliseconds, less than its 100 ms period)
+    sampler.busy_until_sampled(lambda: h.advance(8))
     barrier(dist)
     done = h.advance(args.steps)
     dev_ms, launches = h.run_stats()
+    sampler.busy_until_sampled(lambda: h.advance(8), more=1)  # and once after it
     clocks = sampler.stop()
     barrier(dist)
     assert done == args.steps, f"only {done} of {args.steps} steps ran"
@@ -390,7 +413,7 @@ def slab_arm(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(S.local.stream_ptr())
     sampler = ClockSampler(local_rank)
     sampler.start()
-    S.advance(8)  # untimed pre-roll while the clock sampler starts
+    sampler.busy_until_sampled(lambda: S.advance(8))  # untimed steps until the sampler records
     barrier(dist)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     before = S.steps
@@ -399,6 +422,7 @@ def slab_arm(args, rank, world, local_rank):
     e1.record(stream)
     e1.synchronize()
     _, steps_now, _ = S.sync()
+    sampler.busy_until_sampled(lambda: S.advance(8), more=1)
     clocks = sampler.stop()
     dev_ms = e0.elapsed_time(e1)
     assert steps_now - before == args.steps, f"only {steps_now - before} of {args.steps} steps ran"
@@ -412,13 +436,14 @@ def slab_arm(args, rank, world, local_rank):
     # back, the owned rows downloaded at the end
     pin_in = torch.empty((S.l_hi - S.l_lo, n, 4), dtype=torch.float64, pin_memory=True).numpy()
     pin_in[:] = rows(S.l_lo, S.l_hi)
+    out_rows = torch.empty((4, S.hi - S.lo, n), dtype=torch.float64, pin_memory=True).numpy()
     barrier(dist)
     t0 = time.perf_counter()
     S.set_local_state(pin_in)
     for _ in range(args.steps):
         S.enqueue_steps(1)
         S.sync()
-    out_rows = S.owned_rows()
+    S.owned_planes(out=out_rows)
     e2e_s = allreduce_max(dist, time.perf_counter() - t0)
     S.close()
     e2e = n * ny * args.steps / e2e_s

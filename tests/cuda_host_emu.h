@@ -128,6 +128,9 @@ void launch(dim3 grid, dim3 block, bool threaded, F body)
 
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+// correctly rounded products and sums that the compiler may not contract
+static inline double __dmul_rn(double a, double b) { return a * b; }
+static inline double __dadd_rn(double a, double b) { return a + b; }
 // sm_100's two-wide FP32 instructions: two correctly rounded operations
 static inline float2 __fadd2_rn(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 static inline float2 __fmul2_rn(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }

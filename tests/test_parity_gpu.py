@@ -113,7 +113,8 @@ def test_fma_within_tolerance_after_every_step_of_the_quadrant_workload(pkg, ora
     """The 400x400 workload compared step by step: after each of its 620
     steps the product build (FP64, shared reciprocals, FMA) stays within the
     relative L1 tolerance of the oracle in every field, and its step size
-    within a few ulp of the oracle's."""
+    within 1e-12 of the oracle's (the states differ at the 1e-11 level, and
+    so do their wave-speed maxima)."""
     z, manifest = golden
     m = manifest["quad_outflow_400x400_seed0"]
     kw = {k: m[k] for k in RUN_KEYS}
@@ -128,7 +129,7 @@ def test_fma_within_tolerance_after_every_step_of_the_quadrant_workload(pkg, ora
         U, t, dt = r
         assert h.advance(1) == 1, f"the product's loop ended after {k} steps"
         tg, sg, dtg = h.time()
-        assert sg == k + 1 and dtg == pytest.approx(dt, rel=1e-14, abs=0)
+        assert sg == k + 1 and dtg == pytest.approx(dt, rel=1e-12, abs=0)
         err = max(rel_l1(h.get_state(4), U))
         assert err <= REL_L1_TOL, f"step {k + 1}: relative L1 {err}"
         worst = max(worst, err)
