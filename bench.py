@@ -199,21 +199,22 @@ def product_arm(args, rank, world, local_rank):
     prec = pkg.FP32 if args.precision == "fp32" else pkg.FP64
     if prec != pkg.FP64 and not args.kernels_only:
         raise SystemExit("--precision fp32 applies to --kernels-only runs; the full line reports FP32 beside FP64")
+    # the clock sampler starts first, so it is recording by the time the
+    # steps run (the timed region lasts tens of milliseconds, less than its
+    # 100 ms period): samples come from the warm-up, the timed steps and the
+    # steps right after them
+    sampler = ClockSampler(local_rank)
+    sampler.start()
     h = pkg.Handle(n, n)
     h.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
                 CFG["strategy"], prec)
     h.set_state(U0)
     h.advance(args.warmup)
-
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    # untimed steps until the clock sampler has recorded under load (the
-    # timed region lasts tens of milliseconds, less than its 100 ms period)
-    sampler.busy_until_sampled(lambda: h.advance(8))
+    sampler.busy_until_sampled(lambda: h.advance(8), limit_s=1.0)
     barrier(dist)
     done = h.advance(args.steps)
     dev_ms, launches = h.run_stats()
-    sampler.busy_until_sampled(lambda: h.advance(8), more=1)  # and once after it
+    sampler.busy_until_sampled(lambda: h.advance(8), more=1, limit_s=1.0)  # and once after it
     clocks = sampler.stop()
     barrier(dist)
     assert done == args.steps, f"only {done} of {args.steps} steps ran"
@@ -413,7 +414,7 @@ def slab_arm(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(S.local.stream_ptr())
     sampler = ClockSampler(local_rank)
     sampler.start()
-    sampler.busy_until_sampled(lambda: S.advance(8))  # untimed steps until the sampler records
+    sampler.busy_until_sampled(lambda: S.advance(8), limit_s=1.0)  # untimed steps until the sampler records
     barrier(dist)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     before = S.steps
@@ -422,7 +423,7 @@ def slab_arm(args, rank, world, local_rank):
     e1.record(stream)
     e1.synchronize()
     _, steps_now, _ = S.sync()
-    sampler.busy_until_sampled(lambda: S.advance(8), more=1)
+    sampler.busy_until_sampled(lambda: S.advance(8), more=1, limit_s=1.0)
     clocks = sampler.stop()
     dev_ms = e0.elapsed_time(e1)
     assert steps_now - before == args.steps, f"only {steps_now - before} of {args.steps} steps ran"
