@@ -440,9 +440,10 @@ __global__ void __launch_bounds__(NT, MINB) sweep_x_kernel(SweepArgs<Real> a)
     const long long wstride = (long long)gridDim.x * (NT / 32);
     double vmax = 0.0;
     int bad = 0;
-    // the ring serves the first x-sweep; the final one (which also reads
-    // branch A and reduces over the block) was measured slower with it
-    constexpr int RING = (!FINAL && (sizeof(Real) == 4 || sizeof(Real) == 8)) ? FVM2D_X_RING : 0;
+    // the ring serves the first FP64 x-sweep; the final one (which also
+    // reads branch A and reduces over the block) and the issue-bound FP32
+    // ones were measured slower with it
+    constexpr int RING = (!FINAL && sizeof(Real) == 8) ? FVM2D_X_RING : 0;
     if constexpr (RING > 0) {
         __shared__ Real ring[(NT / 32) * kXRingChunks * 128];
         Real *mine = ring + (threadIdx.x / 32) * kXRingChunks * 128;
