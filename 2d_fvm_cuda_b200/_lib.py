@@ -66,6 +66,7 @@ SIGNATURES = [
     ("fvm2d_measure_fp64_peak", ctypes.c_int, [_dp, _dp]),
     ("fvm2d_eval_reciprocals", ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp]),
     ("fvm2d_set_fixed_dt", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("fvm2d_set_vjp_overlap", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fvm2d_jvp", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
     ("fvm2d_forward", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     ("fvm2d_vjp", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
@@ -326,6 +327,11 @@ class Handle:
     # -- differentiation (fixed dt; forward/vjp on FP64 or FP32, jvp on FP64) --
     def set_fixed_dt(self, dt: float) -> None:
         check(self.lib.fvm2d_set_fixed_dt(self.h, float(dt)))
+
+    def set_vjp_overlap(self, on: bool) -> None:
+        """Two tape buffers in vjp(), the next segment recomputed while the
+        current one is reversed (the default), or one buffer taking turns."""
+        check(self.lib.fvm2d_set_vjp_overlap(self.h, int(bool(on))))
 
     def jvp(self, nsteps: int, tangent) -> np.ndarray:
         """Advances nsteps carrying `tangent`; returns the final tangent."""

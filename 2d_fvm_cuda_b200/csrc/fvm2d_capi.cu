@@ -143,17 +143,26 @@ struct fvm2d_solver {
     // differentiation workspaces (allocated on first use)
     void *dual = nullptr;         // 3 state buffers of dual numbers (jvp)
     char *ckpt = nullptr;         // checkpoints of fvm2d_forward (states of the build's type)
-    char *tape = nullptr;         // one segment's steps, recomputed by fvm2d_vjp (or every step, written
-                                  // by a full-tape fvm2d_forward): per step its input state, X(U), Y(U)
-                                  // and the fluxes of its four sweeps
+    char *tape = nullptr;         // one or two segments' steps, recomputed by fvm2d_vjp (or every step,
+                                  // written by a full-tape fvm2d_forward): per step its input state, X(U),
+                                  // Y(U) and the fluxes of its four sweeps
     char *adj = nullptr;          // adjoint work: 2 adjoints, 3 work states, the saved final state
     size_t ck_bytes = 0, tape_bytes = 0, adj_bytes = 0;
     int ck_count = 0, ck_len = 0, fwd_steps = -1, fwd_precision = -1;
     bool full_tape = false;       // the last fvm2d_forward kept every step's tape
-    // fvm2d_vjp's graphs for a full segment: its taped recompute, and its
-    // reverse starting from either adjoint buffer; built for vjp_len steps
-    cudaGraphExec_t vjp_graph[3] = {nullptr, nullptr, nullptr};
-    int vjp_len = 0;
+    // fvm2d_vjp's graphs for a full segment: its taped recompute into tape
+    // buffer b ([b]), and its reverse from tape buffer b starting from
+    // adjoint buffer a ([2 + 2b + a]); built for vjp_len steps and vjp_bufs
+    // tape buffers
+    cudaGraphExec_t vjp_graph[6] = {};
+    int vjp_len = 0, vjp_bufs = 0;
+    bool last_taped = false;      // the checkpointed forward taped its last segment (fvm2d_vjp skips its recompute)
+    bool vjp_overlap = true;      // fvm2d_set_vjp_overlap: two tape buffers where they fit
+    // with two tape buffers fvm2d_vjp recomputes the next segment on `aux`
+    // while the current one is reversed on `stream`; vjp_ev[b] marks tape
+    // buffer b filled, vjp_ev[2 + b] free again, vjp_ev[4] the start
+    cudaStream_t aux = nullptr;
+    cudaEvent_t vjp_ev[5] = {};
     std::vector<double> ck_t;     // time at each checkpoint
     double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
     double last_device_ms = 0.0;  // CUDA-event time of the last loop on the stream
@@ -198,6 +207,7 @@ struct fvm2d_solver {
         }
         graph_variant = -1;
         drop_vjp_graphs();
+        last_taped = false;  // taped with the former parameters
         if (full_tape) {  // a parameter changed: the tape no longer belongs to this solver's step
             full_tape = false;
             fwd_steps = -1;
@@ -211,6 +221,7 @@ struct fvm2d_solver {
             g = nullptr;
         }
         vjp_len = 0;
+        vjp_bufs = 0;
     }
 
     // Captures what `enqueue` puts on the stream into *out.
@@ -399,6 +410,12 @@ int fvm2d_destroy(fvm2d_solver *s)
     if (s->adj) cudaFree(s->adj);
     if (s->ev_begin) cudaEventDestroy(s->ev_begin);
     if (s->ev_end) cudaEventDestroy(s->ev_end);
+    for (auto &e : s->vjp_ev)
+        if (e) cudaEventDestroy(e);
+    if (s->aux) {
+        cudaStreamSynchronize(s->aux);
+        cudaStreamDestroy(s->aux);
+    }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FVM2D_OK;
@@ -995,6 +1012,15 @@ int fvm2d_profile_kernels(fvm2d_solver *s, int nsteps, double *kernel_ms, int *s
 
 // ---- differentiation -------------------------------------------------------
 
+int fvm2d_set_vjp_overlap(fvm2d_solver *s, int on)
+{
+    if (int rc = check(s)) return rc;
+    s->vjp_overlap = on != 0;
+    s->drop_vjp_graphs();
+    s->last_taped = false;  // the buffer it sits in follows the buffer count
+    return FVM2D_OK;
+}
+
 int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt)
 {
     if (int rc = check(s)) return rc;
@@ -1107,30 +1133,53 @@ int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tan
 
 constexpr int kTapeStates = 7;  // per taped step: U, X(U), Y(U), the fluxes of its 4 sweeps
 
-// State q of taped step j.
-static char *tape_at(const fvm2d_solver *s, int j, int q, size_t sb)
+// State q of taped step j in tape buffer `buf` (buffers of ck_len steps).
+static char *tape_at(const fvm2d_solver *s, int buf, int j, int q, size_t sb)
 {
-    return s->tape + ((size_t)j * kTapeStates + q) * sb;
+    return s->tape + (((size_t)buf * s->ck_len + j) * kTapeStates + q) * sb;
 }
 
-// Enqueues m taped steps (control planned) from the state in tape slot 0:
-// step j reads slot j's input state, fills the rest of slot j and writes its
-// result as slot j+1's input state, the last step's into U.
-static int taped_steps(fvm2d_solver *s, const LaunchConfig &c, int m)
+// Enqueues on `st` m taped steps (control planned) from the state in slot 0
+// of tape buffer `buf`: step j reads slot j's input state, fills the rest of
+// slot j and writes its result as slot j+1's input state, the last step's
+// into U.
+static int taped_steps(fvm2d_solver *s, const LaunchConfig &c, int m, int buf, cudaStream_t st)
 {
     const size_t sb = state_bytes_of(s);
     auto taped_step = is_fp32(s->precision) ? fvm2d::fp32::enqueue_step_taped : fvm2d::fp64::enqueue_step_taped;
     for (int j = 0; j < m; ++j) {
         LaunchConfig cj = c;
-        cj.U = tape_at(s, j, 0, sb);
-        cj.A = tape_at(s, j, 1, sb);
-        cj.B = tape_at(s, j, 2, sb);
-        void *const flux[4] = {tape_at(s, j, 3, sb), tape_at(s, j, 4, sb), tape_at(s, j, 5, sb),
-                               tape_at(s, j, 6, sb)};
-        void *const out = j + 1 < m ? static_cast<void *>(tape_at(s, j + 1, 0, sb)) : static_cast<void *>(s->U);
-        CK(taped_step(cj, s->stream, flux, out));
+        cj.U = tape_at(s, buf, j, 0, sb);
+        cj.A = tape_at(s, buf, j, 1, sb);
+        cj.B = tape_at(s, buf, j, 2, sb);
+        void *const flux[4] = {tape_at(s, buf, j, 3, sb), tape_at(s, buf, j, 4, sb), tape_at(s, buf, j, 5, sb),
+                               tape_at(s, buf, j, 6, sb)};
+        void *const out =
+            j + 1 < m ? static_cast<void *>(tape_at(s, buf, j + 1, 0, sb)) : static_cast<void *>(s->U);
+        CK(taped_step(cj, st, flux, out));
     }
     return FVM2D_OK;
+}
+
+// The control record of a recomputed segment: time t, nothing committed, the
+// fixed step dt planned.  Written by a kernel on the recompute's stream, so
+// each segment's record travels with its own launch (a host-side record
+// copied asynchronously could be overwritten by the next segment's before
+// the copy runs).
+__global__ void segment_control(StepControl *c, double t, double dt)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        c->t = t;
+        c->dt = dt;
+        c->smax_last = 0.0;
+        c->smax_bits = 0ull;
+        c->steps = 0;
+        c->step_limit = INT_MAX;
+        c->active = 1;
+        c->done = 0;
+        c->ticket = 0u;
+        c->first_bad = 0;
+    }
 }
 
 // fvm2d_forward with FVM2D_FULL_TAPE: the forward steps are the taped ones.
@@ -1162,8 +1211,8 @@ static int forward_full_tape(fvm2d_solver *s, int nsteps)
     const LaunchConfig c = s->config();
     CK(s->need_init ? kVariants[s->precision].init(c, s->stream) : kVariants[s->precision].plan(c, s->stream));
     s->need_init = false;
-    CK(cudaMemcpyAsync(tape_at(s, 0, 0, sb), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-    if (int rc = taped_steps(s, c, nsteps)) return rc;
+    CK(cudaMemcpyAsync(tape_at(s, 0, 0, 0, sb), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+    if (int rc = taped_steps(s, c, nsteps, 0, s->stream)) return rc;
     CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     s->ck_count = 1;
@@ -1172,6 +1221,114 @@ static int forward_full_tape(fvm2d_solver *s, int nsteps)
     s->fwd_precision = s->precision;
     s->full_tape = true;
     s->total_steps += nsteps;
+    return FVM2D_OK;
+}
+
+// Steps of checkpoint segment k when nsteps are split into `count` segments
+// of at most len steps: the first one takes the remainder, so the last one,
+// which the forward tapes and the reverse meets first, is a full segment
+// (and its recompute never waits on a shorter reverse).
+static int segment_steps(int nsteps, int len, int count, int k)
+{
+    return k == 0 ? nsteps - (count - 1) * len : len;
+}
+
+constexpr int kAdjStates = 6;  // adjoint workspace: two adjoints, three work states, the saved final state
+
+// The adjoint step's launch parameters for this handle; the tape and
+// adjoint pointers are filled per step.
+static fvm2d::AdjointLaunch adjoint_launch_of(const fvm2d_solver *s, size_t sb)
+{
+    fvm2d::AdjointLaunch L{};
+    L.nx = s->nx;
+    L.ny = s->ny;
+    L.pitch = s->pitch;
+    L.plane = s->plane;
+    L.strategy = s->strategy;
+    const LaunchConfig c = s->config();
+    L.hx = c.hx;
+    L.hy = c.hy;
+    L.rhx = c.rhx;
+    L.rhy = c.rhy;
+    L.alpha = s->alpha;
+    L.gamma = s->gamma;
+    L.dt = s->fixed_dt;
+    for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * sb;
+    return L;
+}
+
+// Enqueues on `st` the reverse of m steps taped in buffer `buf`, starting
+// from adjoint buffer `from` (0 or 1 of the workspace); the result lands in
+// `from` for even m, in the other buffer for odd m.
+static int reverse_steps(fvm2d_solver *s, int m, int buf, int from, cudaStream_t st)
+{
+    const size_t sb = state_bytes_of(s);
+    auto adjoint_step = is_fp32(s->precision) ? fvm2d::adj32::adjoint_step : fvm2d::adj::adjoint_step;
+    fvm2d::AdjointLaunch L = adjoint_launch_of(s, sb);
+    char *a = s->adj + from * sb, *b = s->adj + (1 - from) * sb;
+    for (int j = m - 1; j >= 0; --j) {
+        L.U = tape_at(s, buf, j, 0, sb);
+        L.A1 = tape_at(s, buf, j, 1, sb);
+        L.B1 = tape_at(s, buf, j, 2, sb);
+        for (int q = 0; q < 4; ++q) L.flux[q] = tape_at(s, buf, j, 3 + q, sb);
+        L.lb_out = a;
+        L.lb_in = b;
+        CK(adjoint_step(L, st));
+        std::swap(a, b);
+    }
+    return FVM2D_OK;
+}
+
+// Workspace of a checkpointed reverse (ck_count segments of ck_len steps):
+// the adjoint states and the tape buffers -- two where the device has room
+// for the second (segment k-1 is then recomputed on the aux stream while
+// segment k is reversed), else one -- with the aux stream, its events and
+// the graphs of a full segment's recompute and reverse.  *bufs is 1 or 2.
+static int vjp_workspace(fvm2d_solver *s, int *bufs)
+{
+    const size_t sb = state_bytes_of(s);
+    const size_t seg_bytes = (size_t)s->ck_len * kTapeStates * sb;
+    *bufs = 1;
+    if (s->ck_count > 1 && s->vjp_overlap) {
+        if (s->tape_bytes >= 2 * seg_bytes) {
+            *bufs = 2;
+        } else {
+            size_t free_b = 0, total_b = 0;
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            const size_t margin = (size_t)256 << 20;  // left to the rest of the process
+            const size_t adj_need = s->adj_bytes >= kAdjStates * sb ? 0 : kAdjStates * sb;
+            if (2 * seg_bytes + adj_need + margin <= free_b + s->tape_bytes) *bufs = 2;
+        }
+    }
+    bool grew_tape, grew_adj;
+    if (int rc = ensure(s->tape, s->tape_bytes, *bufs * seg_bytes, grew_tape)) return rc;
+    if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
+    if (grew_tape || grew_adj) s->drop_vjp_graphs();
+    if (grew_tape) s->last_taped = false;
+    if (*bufs == 2 && !s->aux) {
+        // default priority: the recompute fills the SM room the reverse's
+        // blocks leave (measured: at the device's higher priority the VJP
+        // took 1% longer)
+        CK(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+        for (auto &e : s->vjp_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    // graphs of a full segment, kept while the handle's parameters, build and
+    // buffers stay the same
+    if (s->ck_count > 1 && (s->vjp_len != s->ck_len || s->vjp_bufs != *bufs)) {
+        s->drop_vjp_graphs();
+        CK(is_fp32(s->precision) ? fvm2d::adj32::adjoint_prepare() : fvm2d::adj::adjoint_prepare());
+        const LaunchConfig c = s->config();
+        const int len = s->ck_len;
+        for (int b = 0; b < *bufs; ++b) {
+            if (int rc = s->capture(&s->vjp_graph[b], [&] { return taped_steps(s, c, len, b, s->stream); }))
+                return rc;
+            for (int a = 0; a < 2; ++a)
+                if (int rc = s->capture(&s->vjp_graph[2 + 2 * b + a], [&] { return reverse_steps(s, len, b, a, s->stream); }))
+                    return rc;
+        }
+        s->vjp_len = len;
+        s->vjp_bufs = *bufs;
+    }
     return FVM2D_OK;
 }
 
@@ -1190,6 +1347,16 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     bool grew;
     if (int rc = ensure(s->ckpt, s->ck_bytes, (size_t)count * sb, grew)) return rc;
     if (int rc = s->build_graphs()) return rc;  // the step graphs of the fixed-dt build
+    s->fwd_steps = -1;
+    s->full_tape = false;
+    s->last_taped = false;
+    s->ck_count = count;
+    s->ck_len = len;
+    // the last segment, the first one the reverse needs, is taped as it runs
+    // (as revolve schedules do), so fvm2d_vjp does not recompute it
+    int bufs = 1;
+    if (count > 1)
+        if (int rc = vjp_workspace(s, &bufs)) return rc;
     StepControl *h = s->ctl_h;
     h->step_limit = INT_MAX;
     h->done = 0;
@@ -1203,7 +1370,18 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     for (int k = 0; k < count; ++k) {
         s->ck_t[k] = t;
         CK(cudaMemcpyAsync(s->ckpt + k * sb, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-        const int m = (k + 1) * len <= nsteps ? len : nsteps - k * len;
+        const int m = segment_steps(nsteps, len, count, k);
+        if (count > 1 && k == count - 1) {
+            const int b = k % bufs;
+            CK(cudaMemcpyAsync(tape_at(s, b, 0, 0, sb), s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
+            if (m == s->vjp_len) {
+                CK(cudaGraphLaunch(s->vjp_graph[b], s->stream));
+            } else if (int rc = taped_steps(s, c, m, b, s->stream)) {
+                return rc;
+            }
+            for (int q = 0; q < m; ++q) t = t + s->fixed_dt;
+            continue;
+        }
         for (int j = 0; j < m;) {
             const int which = m - j >= fvm2d_solver::kGraphSteps[0] ? 0 : 1;
             CK(cudaGraphLaunch(s->graph[which], s->stream));
@@ -1213,11 +1391,9 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
     }
     CK(cudaMemcpyAsync(h, s->ctl, sizeof(StepControl), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    s->ck_count = count;
-    s->ck_len = len;
     s->fwd_steps = nsteps;
     s->fwd_precision = s->precision;
-    s->full_tape = false;
+    s->last_taped = count > 1;
     s->total_steps += nsteps;
     return FVM2D_OK;
 }
@@ -1231,91 +1407,82 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
         return fail(FVM2D_ERR_STATE, "fvm2d_vjp reverses the last fvm2d_forward of this build: call it first");
     if (!cotangent_in || !cotangent_out) return fail(FVM2D_ERR_INVALID, "null cotangent pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
-    const bool f32 = is_fp32(s->precision);
     const size_t sb = state_bytes_of(s);
-    constexpr int kAdjStates = 6;  // two adjoints, three work states, the saved final state
-    bool grew_tape, grew_adj;
-    if (int rc = ensure(s->tape, s->tape_bytes, (size_t)s->ck_len * kTapeStates * sb, grew_tape)) return rc;
-    if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
-    if (grew_tape || grew_adj) s->drop_vjp_graphs();
-    char *const adj0 = s->adj, *const adj1 = s->adj + sb, *const saved = s->adj + 5 * sb;
-    char *lam = adj0, *lam2 = adj1;
-    fvm2d::AdjointLaunch L;
-    L.nx = s->nx;
-    L.ny = s->ny;
-    L.pitch = s->pitch;
-    L.plane = s->plane;
-    L.strategy = s->strategy;
-    const LaunchConfig c = s->config();
-    L.hx = c.hx;
-    L.hy = c.hy;
-    L.rhx = c.rhx;
-    L.rhy = c.rhy;
-    L.alpha = s->alpha;
-    L.gamma = s->gamma;
-    L.dt = s->fixed_dt;
-    for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * sb;
+    int bufs = 1;
+    if (s->full_tape) {
+        bool grew_adj;
+        if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
+        if (grew_adj) s->drop_vjp_graphs();
+    } else if (int rc = vjp_workspace(s, &bufs)) {
+        return rc;
+    }
+    char *const saved = s->adj + 5 * sb;
+    int lam = 0;  // adjoint buffer holding the current adjoint
     const StepControl after = *s->ctl_h;
     CK(cudaMemcpyAsync(saved, s->U, sb, cudaMemcpyDeviceToDevice, s->stream));
-    if (int rc = cells_to_planes(s, cotangent_in, stride, lam)) return rc;
-    StepControl *h = s->ctl_h;
-    auto tape = [&](int j, int q) { return tape_at(s, j, q, sb); };
-    auto adjoint_step = f32 ? fvm2d::adj32::adjoint_step : fvm2d::adj::adjoint_step;
-    // the taped recompute of m steps from the state in tape slot 0, and the
-    // reverse of m steps from adjoint buffer `from` (the result lands in
-    // `from` for even m)
-    auto recompute = [&](int m) -> int { return taped_steps(s, c, m); };
-    auto reverse = [&](int m, char *from) -> int {
-        char *a = from, *b = from == adj0 ? adj1 : adj0;
-        for (int j = m - 1; j >= 0; --j) {
-            L.U = tape(j, 0);
-            L.A1 = tape(j, 1);
-            L.B1 = tape(j, 2);
-            for (int q = 0; q < 4; ++q) L.flux[q] = tape(j, 3 + q);
-            L.lb_out = a;
-            L.lb_in = b;
-            CK(adjoint_step(L, s->stream));
-            std::swap(a, b);
-        }
-        return FVM2D_OK;
-    };
-    // graphs of a full segment, kept while the handle's parameters, build and
-    // buffers stay the same
-    if (!s->full_tape && s->vjp_len != s->ck_len && s->ck_count > 1) {
-        s->drop_vjp_graphs();
-        CK(f32 ? fvm2d::adj32::adjoint_prepare() : fvm2d::adj::adjoint_prepare());
-        const int len = s->ck_len;
-        if (int rc = s->capture(&s->vjp_graph[0], [&] { return recompute(len); })) return rc;
-        if (int rc = s->capture(&s->vjp_graph[1], [&] { return reverse(len, adj0); })) return rc;
-        if (int rc = s->capture(&s->vjp_graph[2], [&] { return reverse(len, adj1); })) return rc;
-        s->vjp_len = len;
-    }
-    for (int k = s->ck_count - 1; k >= 0; --k) {
-        const int m = (k + 1) * s->ck_len <= s->fwd_steps ? s->ck_len : s->fwd_steps - k * s->ck_len;
-        if (s->full_tape) {  // the forward taped every step: reverse only
-            if (int rc = reverse(m, lam)) return rc;
-            if (m & 1) std::swap(lam, lam2);
-            continue;
-        }
-        // recompute the segment from its checkpoint, taping every step
-        CK(cudaMemcpyAsync(tape(0, 0), s->ckpt + k * sb, sb, cudaMemcpyDeviceToDevice, s->stream));
-        std::memset(h, 0, sizeof(StepControl));
-        h->t = s->ck_t[k];
-        h->step_limit = INT_MAX;
-        if (int rc = s->upload_control()) return rc;
-        CK(kVariants[s->precision].plan(c, s->stream));
-        if (m == s->vjp_len) {
-            CK(cudaGraphLaunch(s->vjp_graph[0], s->stream));
-            CK(cudaGraphLaunch(s->vjp_graph[lam == adj0 ? 1 : 2], s->stream));
+    if (int rc = cells_to_planes(s, cotangent_in, stride, s->adj)) return rc;
+    const int count = s->ck_count;
+    auto seg_len = [&](int k) { return segment_steps(s->fwd_steps, s->ck_len, count, k); };
+    if (s->full_tape) {  // the forward taped every step: reverse only
+        if (int rc = reverse_steps(s, s->fwd_steps, 0, lam, s->stream)) return rc;
+        lam ^= s->fwd_steps & 1;
+    } else {
+        // segment k is taped in buffer k % bufs
+        auto recompute_segment = [&](int k, cudaStream_t st) -> int {
+            if (k == count - 1 && s->last_taped) return FVM2D_OK;  // taped by the forward
+            const int m = seg_len(k), b = k % bufs;
+            CK(cudaMemcpyAsync(tape_at(s, b, 0, 0, sb), s->ckpt + k * sb, sb, cudaMemcpyDeviceToDevice, st));
+            segment_control<<<1, 32, 0, st>>>(s->ctl, s->ck_t[k], s->fixed_dt);
+            CK(cudaGetLastError());
+            if (m == s->vjp_len) {
+                CK(cudaGraphLaunch(s->vjp_graph[b], st));
+            } else if (int rc = taped_steps(s, s->config(), m, b, st)) {
+                return rc;
+            }
+            return FVM2D_OK;
+        };
+        auto reverse_segment = [&](int k, cudaStream_t st) -> int {
+            const int m = seg_len(k), b = k % bufs;
+            if (m == s->vjp_len) {
+                CK(cudaGraphLaunch(s->vjp_graph[2 + 2 * b + lam], st));
+            } else if (int rc = reverse_steps(s, m, b, lam, st)) {
+                return rc;
+            }
+            lam ^= m & 1;
+            return FVM2D_OK;
+        };
+        if (bufs == 1) {
+            for (int k = count - 1; k >= 0; --k) {
+                if (int rc = recompute_segment(k, s->stream)) return rc;
+                if (int rc = reverse_segment(k, s->stream)) return rc;
+            }
         } else {
-            if (int rc = recompute(m)) return rc;
-            if (int rc = reverse(m, lam)) return rc;
+            // aux: recompute(K-1), recompute(K-2), ...; stream: reverse(K-1),
+            // reverse(K-2), ...  reverse(k) waits for recompute(k) (buffer
+            // filled); recompute(k-1) waits for reverse(k+1), the last user
+            // of its buffer.  The recomputes own the control record and U
+            // (restored from `saved` below, after the last wait).
+            cudaEvent_t *const filled = s->vjp_ev, *const freed = s->vjp_ev + 2, start = s->vjp_ev[4];
+            CK(cudaEventRecord(start, s->stream));
+            CK(cudaStreamWaitEvent(s->aux, start, 0));
+            if (int rc = recompute_segment(count - 1, s->aux)) return rc;
+            CK(cudaEventRecord(filled[(count - 1) % 2], s->aux));
+            for (int k = count - 1; k >= 0; --k) {
+                CK(cudaStreamWaitEvent(s->stream, filled[k % 2], 0));
+                if (int rc = reverse_segment(k, s->stream)) return rc;
+                CK(cudaEventRecord(freed[k % 2], s->stream));
+                if (k > 0) {
+                    if (k + 1 < count) CK(cudaStreamWaitEvent(s->aux, freed[(k + 1) % 2], 0));
+                    if (int rc = recompute_segment(k - 1, s->aux)) return rc;
+                    CK(cudaEventRecord(filled[(k - 1) % 2], s->aux));
+                }
+            }
         }
-        if (m & 1) std::swap(lam, lam2);
+        s->last_taped = false;  // its buffer has been reused (or will be by the next call)
     }
-    if (int rc = planes_to_cells(s, lam, cotangent_out, stride)) return rc;
+    if (int rc = planes_to_cells(s, s->adj + lam * sb, cotangent_out, stride)) return rc;
     CK(cudaMemcpyAsync(s->U, saved, sb, cudaMemcpyDeviceToDevice, s->stream));
-    *h = after;
+    *s->ctl_h = after;
     if (int rc = s->upload_control()) return rc;
     CK(cudaStreamSynchronize(s->stream));
     return FVM2D_OK;

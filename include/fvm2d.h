@@ -284,7 +284,8 @@ int fvm2d_set_fixed_dt(fvm2d_solver *s, double dt);
 int fvm2d_jvp(fvm2d_solver *s, int nsteps, const double *tangent_in, double *tangent_out, int stride);
 
 /* Advances the state nsteps steps keeping `checkpoints` evenly spaced
- * copies of it (sqrt(nsteps) is the usual choice) for fvm2d_vjp.
+ * copies of it (sqrt(nsteps) is the usual choice) for fvm2d_vjp; the last
+ * segment, the first one the reverse needs, is taped as it runs.
  * checkpoints = FVM2D_FULL_TAPE keeps instead the whole tape: every step's
  * input state, X(U), Y(U) and interface fluxes, 7 states per step (8.4 MB x 7
  * per step at 512^2 in FP64), written by the forward steps themselves, so
@@ -303,6 +304,13 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints);
  * layout, precision, row frame, step size) after a full-tape forward
  * discards its tape. */
 int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out, int stride);
+
+/* With checkpoints, fvm2d_forward tapes its last segment as it runs and
+ * fvm2d_vjp recomputes the others.  on != 0 (the default): where the device
+ * has room for two segments' tapes, segment k-1 is recomputed on a second
+ * stream while segment k is reversed; 0: one tape buffer, recompute and
+ * reverse taking turns (half the tape memory).  The gradient is the same. */
+int fvm2d_set_vjp_overlap(fvm2d_solver *s, int on);
 
 /* ---- batched form (no reference counterpart) -------------------------------
  * Many independent problems of different sizes advance together: every stage

@@ -21,6 +21,9 @@ can cross a switch.
 * A full-tape forward (every step taped, nothing recomputed in the VJP) gives
   the checkpointed run's state and cotangent, serves several VJPs, and is
   discarded when a parameter changes.
+* The checkpointed reverse's two schedules (next segment recomputed on a
+  second stream while the current one is reversed, or both in turn on one
+  stream) and the full tape give one gradient on every preset.
 """
 import numpy as np
 import pytest
@@ -141,6 +144,40 @@ def test_dot_product_many_steps_with_checkpoints(pkg, steps, checkpoints):
     hd.close()
     a, b = np.sum(jv * wv), np.sum(v * vj)
     assert abs(a - b) <= 1e-10 * max(abs(a), abs(b)), (a, b)
+
+
+# Several checkpoint segments, the first one short, on every preset (the
+# double-Mach fill depends on the time, so each recomputed segment must start
+# from its own checkpoint's time).  The forward tapes its last segment as it
+# runs; the VJP recomputes the others on a second stream while reversing
+# (overlap on) or in turn on one stream with one tape buffer (overlap off).
+# Both schedules, a second VJP of the same forward (which recomputes the
+# segment the forward taped) and the full tape (whose forward runs every step
+# in order) give one gradient, up to the reordered sums of the ghost
+# transpose's atomics.  (The dot-product identity with the JVP is checked on
+# smooth data above: over many steps of these discontinuous states the
+# dual-number forward, rounded differently, can take another limiter branch.)
+@pytest.mark.parametrize("strategy", [0, 1, 2, 3, 4, 5, 6])
+def test_checkpoint_schedules_agree_every_preset(pkg, oracle, strategy):
+    n, steps, checkpoints = 48, 23, 5  # 5 segments: the first of 3 steps, the others of 5
+    U = oracle.ghost(pkg.scenarios.seeded_four_quadrant(n, 40, 110 + strategy), strategy)
+    dt = fixed_dt(pkg, U, 1.0 / n) * 0.5
+    wv = np.random.default_rng(100 + strategy).standard_normal(U.shape)
+    hd = handle(pkg, U, 1.0, 40 / n, dt, strategy)
+    grads = []
+    for overlap in (True, False):
+        hd.set_vjp_overlap(overlap)
+        hd.set_state(U)
+        hd.forward(steps, checkpoints)
+        grads.append(hd.vjp(wv))
+        grads.append(hd.vjp(wv))
+    hd.set_state(U)
+    hd.forward(steps, pkg.FULL_TAPE)
+    ref = hd.vjp(wv)
+    hd.close()
+    for k, g in enumerate(grads):
+        rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+        assert rel <= 1e-12, (k, rel)
 
 
 def test_gradient_of_density_objective_matches_finite_differences(pkg):
