@@ -15,6 +15,6 @@ The package directory name starts with a digit, so import it with
   workloads).
 """
 from . import ensemble, scenarios, slab  # noqa: F401
-from ._lib import (FP32, FP64, FP64_REFORDER, FP64_STRICT, FULL_TAPE, LIB_PATH, Batch, FVM2DError,  # noqa: F401
-                   Handle, load, measure_fp64_peak)
+from ._lib import (FP32, FP32_RESIDUAL, FP64, FP64_REFORDER, FP64_STRICT, FULL_TAPE, LIB_PATH, Batch,  # noqa: F401
+                   FVM2DError, Handle, load, measure_fp64_peak)
 from .solver import RGRP_2D_CUDA, ghostCellStrategy, precision  # noqa: F401

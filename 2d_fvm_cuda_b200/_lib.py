@@ -15,7 +15,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libfvm2d.so")
 
 FVM2D_OK, FVM2D_ERR_INVALID, FVM2D_ERR_CUDA, FVM2D_ERR_STATE = 0, 1, 2, 3
-FP64, FP64_STRICT, FP64_REFORDER, FP32 = 0, 1, 2, 3
+FP64, FP64_STRICT, FP64_REFORDER, FP32, FP32_RESIDUAL = 0, 1, 2, 3, 4
 FULL_TAPE = 0  # fvm2d_forward(checkpoints=FULL_TAPE): tape every step, no recompute in vjp
 
 _dp = ctypes.POINTER(ctypes.c_double)

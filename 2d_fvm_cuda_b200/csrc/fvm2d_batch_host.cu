@@ -306,9 +306,11 @@ struct fvm2d_batch {
             const long long n = 4 * plane(p);
             double *U = base + off[p], *S = base + off[p] + 4 * plane(p);
             if (to == FVM2D_FP32)
-                fvm2d::convert_planes<double, float><<<148 * 4, 256, 0, stream>>>(U, reinterpret_cast<float *>(S), n);
+                fvm2d::convert_planes<<<148 * 4, 256, 0, stream>>>(fvm2d::Planes<double>{U},
+                                                                    fvm2d::Planes<float>{reinterpret_cast<float *>(S)}, n);
             else
-                fvm2d::convert_planes<float, double><<<148 * 4, 256, 0, stream>>>(reinterpret_cast<const float *>(U), S, n);
+                fvm2d::convert_planes<<<148 * 4, 256, 0, stream>>>(fvm2d::Planes<float>{reinterpret_cast<float *>(U)},
+                                                                    fvm2d::Planes<double>{S}, n);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(U, S, n * (to == FVM2D_FP32 ? sizeof(float) : sizeof(double)), cudaMemcpyDeviceToDevice,
                                stream));
@@ -473,11 +475,11 @@ int fvm2d_batch_set_state(fvm2d_batch *b, int p, const double *cells, int stride
     const cudaMemcpyKind kind = fvm2d::is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(S, cells, bytes, kind, b->stream));
     if (b->precision == FVM2D_FP32)
-        fvm2d::aos_to_soa<float><<<148 * 4, 256, 0, b->stream>>>(S, stride, reinterpret_cast<float *>(U), b->nx[p],
-                                                                  b->ny[p], b->pitch[p], b->plane(p));
+        fvm2d::aos_to_soa<<<148 * 4, 256, 0, b->stream>>>(S, stride, fvm2d::Planes<float>{reinterpret_cast<float *>(U)},
+                                                           b->nx[p], b->ny[p], b->pitch[p], b->plane(p));
     else
-        fvm2d::aos_to_soa<double><<<148 * 4, 256, 0, b->stream>>>(S, stride, U, b->nx[p], b->ny[p], b->pitch[p],
-                                                                   b->plane(p));
+        fvm2d::aos_to_soa<<<148 * 4, 256, 0, b->stream>>>(S, stride, fvm2d::Planes<double>{U}, b->nx[p], b->ny[p],
+                                                           b->pitch[p], b->plane(p));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(b->stream));
     b->have_state[p] = 1;
@@ -492,11 +494,11 @@ int fvm2d_batch_get_state(fvm2d_batch *b, int p, double *cells, int stride)
     if (!b->have_state[p]) return fail(FVM2D_ERR_STATE, "no state has been set for this problem");
     double *U = b->base + b->off[p], *S = U + 4 * b->plane(p);
     if (b->precision == FVM2D_FP32)
-        fvm2d::soa_to_aos<float><<<148 * 4, 256, 0, b->stream>>>(reinterpret_cast<const float *>(U), b->nx[p], b->ny[p],
-                                                                  b->pitch[p], b->plane(p), stride, S);
+        fvm2d::soa_to_aos<<<148 * 4, 256, 0, b->stream>>>(fvm2d::Planes<float>{reinterpret_cast<float *>(U)}, b->nx[p],
+                                                           b->ny[p], b->pitch[p], b->plane(p), stride, S);
     else
-        fvm2d::soa_to_aos<double><<<148 * 4, 256, 0, b->stream>>>(U, b->nx[p], b->ny[p], b->pitch[p], b->plane(p),
-                                                                   stride, S);
+        fvm2d::soa_to_aos<<<148 * 4, 256, 0, b->stream>>>(fvm2d::Planes<double>{U}, b->nx[p], b->ny[p], b->pitch[p],
+                                                           b->plane(p), stride, S);
     CK(cudaGetLastError());
     const size_t bytes = sizeof(double) * (size_t)b->nx[p] * b->ny[p] * stride;
     const cudaMemcpyKind kind = fvm2d::is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

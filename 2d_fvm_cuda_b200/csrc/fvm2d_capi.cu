@@ -85,7 +85,8 @@ struct Variant {
     {fvm2d::ns::prepare, fvm2d::ns::enqueue_init, fvm2d::ns::enqueue_plan, fvm2d::ns::enqueue_step,     \
      fvm2d::ns::enqueue_plan_from}
 const Variant kVariants[] = {FVM2D_VARIANT_ENTRY(fp64), FVM2D_VARIANT_ENTRY(fp64_strict),
-                             FVM2D_VARIANT_ENTRY(fp64_reforder), FVM2D_VARIANT_ENTRY(fp32)};
+                             FVM2D_VARIANT_ENTRY(fp64_reforder), FVM2D_VARIANT_ENTRY(fp32),
+                             FVM2D_VARIANT_ENTRY(fp32r)};
 // the tangent-linear build (dual numbers), used by fvm2d_jvp only
 const Variant kJvp = FVM2D_VARIANT_ENTRY(jvp);
 #undef FVM2D_VARIANT_ENTRY
@@ -107,10 +108,35 @@ __global__ void unpack_dual(const Dual *__restrict__ in, double *__restrict__ v,
     }
 }
 
-// Element type of the state planes for a precision: FP32 stores floats, the
-// FP64 builds doubles.  Host-side states are always doubles.
+// Element type of the state planes for a precision: FP32 stores floats (and
+// FP32_RESIDUAL floats followed by 16-bit residual planes), the FP64 builds
+// doubles.  Host-side states are always doubles.
 bool is_fp32(int precision) { return precision == FVM2D_FP32; }
+bool float_planes(int precision) { return precision == FVM2D_FP32 || precision == FVM2D_FP32_RESIDUAL; }
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// Storage of a precision's state planes: 0 doubles, 1 floats, 2 floats with
+// 16-bit residual planes; and the bytes of one state.
+int storage_of(int precision) { return precision == FVM2D_FP32 ? 1 : precision == FVM2D_FP32_RESIDUAL ? 2 : 0; }
+size_t state_bytes(int precision, long long plane)
+{
+    static const size_t per_element[3] = {sizeof(double), sizeof(float), sizeof(float) + sizeof(unsigned short)};
+    return (size_t)4 * plane * per_element[storage_of(precision)];
+}
+
+// Calls f with the storage policy (fvm2d_split.cuh) of a state buffer of the
+// given precision, for the transfer kernels.
+template <class F>
+void with_planes(int precision, const void *state, long long plane, F &&f)
+{
+    void *U = const_cast<void *>(state);
+    if (precision == FVM2D_FP32)
+        f(fvm2d::Planes<float>{static_cast<float *>(U)});
+    else if (precision == FVM2D_FP32_RESIDUAL)
+        f(fvm2d::split_planes(U, plane));
+    else
+        f(fvm2d::Planes<double>{static_cast<double *>(U)});
+}
 
 } // namespace
 
@@ -327,11 +353,9 @@ int upload(fvm2d_solver *s, const double *cells, int stride)
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
-    if (is_fp32(s->precision))
-        aos_to_soa<float><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, reinterpret_cast<float *>(s->U), s->nx,
-                                                          s->ny, s->pitch, s->plane);
-    else
-        aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, s->U, s->nx, s->ny, s->pitch, s->plane);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        aos_to_soa<<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, st, s->nx, s->ny, s->pitch, s->plane);
+    });
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     s->have_state = true;
@@ -441,17 +465,16 @@ int fvm2d_set_precision(fvm2d_solver *s, int v)
 {
     if (int rc = check(s)) return rc;
     if (!(v >= 0 && v < kNumVariants)) return fail(FVM2D_ERR_INVALID, "unknown precision");
-    if (s->have_state && is_fp32(v) != is_fp32(s->precision)) {
+    if (s->have_state && storage_of(v) != storage_of(s->precision)) {
         // keep the current state: convert its planes to the new storage type
         const long long n = 4 * s->plane;
-        if (is_fp32(v))
-            convert_planes<double, float><<<148 * 4, 256, 0, s->stream>>>(s->U, reinterpret_cast<float *>(s->scratch), n);
-        else
-            convert_planes<float, double><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U),
-                                                                          s->scratch, n);
+        with_planes(s->precision, s->U, s->plane, [&](auto from) {
+            with_planes(v, s->scratch, s->plane, [&](auto to) {
+                convert_planes<<<148 * 4, 256, 0, s->stream>>>(from, to, n);
+            });
+        });
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(s->U, s->scratch, n * (is_fp32(v) ? sizeof(float) : sizeof(double)),
-                           cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaMemcpyAsync(s->U, s->scratch, state_bytes(v, s->plane), cudaMemcpyDeviceToDevice, s->stream));
         CK(cudaStreamSynchronize(s->stream));
     }
     s->precision = v;
@@ -489,11 +512,9 @@ int fvm2d_set_state_planes(fvm2d_solver *s, const double *planes)
     if (int rc = check(s)) return rc;
     if (!planes) return fail(FVM2D_ERR_INVALID, "null state pointer");
     CK(cudaMemcpyAsync(s->scratch, planes, sizeof(double) * 4 * (size_t)s->nx * s->ny, cudaMemcpyDefault, s->stream));
-    if (is_fp32(s->precision))
-        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, 0, s->ny,
-                                                       s->nx, s->scratch);
-    else
-        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, 0, s->ny, s->nx, s->scratch);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        rows_in<<<148 * 4, 256, 0, s->stream>>>(st, s->plane, s->pitch, 0, s->ny, s->nx, s->scratch);
+    });
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     s->have_state = true;
@@ -537,11 +558,9 @@ int fvm2d_get_state(fvm2d_solver *s, double *cells, int stride)
     if (!cells) return fail(FVM2D_ERR_INVALID, "null state pointer");
     if (stride != 4 && stride != 5) return fail(FVM2D_ERR_INVALID, "stride must be 4 or 5 doubles per cell");
     if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
-    if (is_fp32(s->precision))
-        soa_to_aos<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->nx, s->ny, s->pitch,
-                                                          s->plane, stride, s->scratch);
-    else
-        soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        soa_to_aos<<<148 * 4, 256, 0, s->stream>>>(st, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    });
     CK(cudaGetLastError());
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -732,11 +751,9 @@ static int rows_check(fvm2d_solver *s, int j0, int nrows, const void *buf)
 int fvm2d_get_rows(fvm2d_solver *s, int j0, int nrows, double *rows)
 {
     if (int rc = rows_check(s, j0, nrows, rows)) return rc;
-    if (is_fp32(s->precision))
-        rows_out<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->plane, s->pitch, j0,
-                                                        nrows, s->nx, s->scratch);
-    else
-        rows_out<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        rows_out<<<148 * 4, 256, 0, s->stream>>>(st, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    });
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rows, s->scratch, sizeof(double) * 4 * (size_t)nrows * s->nx, cudaMemcpyDefault, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -747,11 +764,9 @@ int fvm2d_set_rows(fvm2d_solver *s, int j0, int nrows, const double *rows)
 {
     if (int rc = rows_check(s, j0, nrows, rows)) return rc;
     CK(cudaMemcpyAsync(s->scratch, rows, sizeof(double) * 4 * (size_t)nrows * s->nx, cudaMemcpyDefault, s->stream));
-    if (is_fp32(s->precision))
-        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, j0, nrows,
-                                                       s->nx, s->scratch);
-    else
-        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        rows_in<<<148 * 4, 256, 0, s->stream>>>(st, s->plane, s->pitch, j0, nrows, s->nx, s->scratch);
+    });
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     return FVM2D_OK;
@@ -775,11 +790,9 @@ int fvm2d_get_rows_async(fvm2d_solver *s, int j0, int nrows, double *rows)
 {
     if (int rc = rows_check(s, j0, nrows, rows)) return rc;
     if (!is_device_pointer(rows)) return fail(FVM2D_ERR_INVALID, "the row buffer must be device memory");
-    if (is_fp32(s->precision))
-        rows_out<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<const float *>(s->U), s->plane, s->pitch, j0,
-                                                        nrows, s->nx, rows);
-    else
-        rows_out<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        rows_out<<<148 * 4, 256, 0, s->stream>>>(st, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    });
     CK(cudaGetLastError());
     return FVM2D_OK;
 }
@@ -788,11 +801,9 @@ int fvm2d_set_rows_async(fvm2d_solver *s, int j0, int nrows, const double *rows)
 {
     if (int rc = rows_check(s, j0, nrows, rows)) return rc;
     if (!is_device_pointer(rows)) return fail(FVM2D_ERR_INVALID, "the row buffer must be device memory");
-    if (is_fp32(s->precision))
-        rows_in<float><<<148 * 4, 256, 0, s->stream>>>(reinterpret_cast<float *>(s->U), s->plane, s->pitch, j0, nrows,
-                                                       s->nx, rows);
-    else
-        rows_in<double><<<148 * 4, 256, 0, s->stream>>>(s->U, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        rows_in<<<148 * 4, 256, 0, s->stream>>>(st, s->plane, s->pitch, j0, nrows, s->nx, rows);
+    });
     CK(cudaGetLastError());
     return FVM2D_OK;
 }
@@ -849,7 +860,7 @@ static int write_frame(fvm2d_solver *s, const char *path)
     if (blocks > 148 * 4) blocks = 148 * 4;
     float *parts = reinterpret_cast<float *>(s->scratch);
     unsigned char *rgb = reinterpret_cast<unsigned char *>(s->scratch) + 4096 * sizeof(float);
-    if (is_fp32(s->precision)) {
+    if (float_planes(s->precision)) {  // the density's FP32 plane (residuals left out of a frame)
         const float *rho = reinterpret_cast<const float *>(s->U);
         fvm2d::io::density_range_blocks<float, NT><<<(int)blocks, NT, 0, s->stream>>>(rho, s->pitch, s->nx, s->ny, parts);
         fvm2d::io::render_density<float><<<148 * 4, 256, 0, s->stream>>>(rho, s->pitch, s->nx, s->ny, parts, (int)blocks,
@@ -1043,7 +1054,7 @@ static int diff_ready(fvm2d_solver *s)
 // Bytes of one state of the current build (4 planes of `plane` values).
 static size_t state_bytes_of(const fvm2d_solver *s)
 {
-    return (size_t)4 * s->plane * (is_fp32(s->precision) ? sizeof(float) : sizeof(double));
+    return state_bytes(s->precision, s->plane);
 }
 
 // (Re)allocates *buf to at least `bytes`; `grew` tells whether it moved.
@@ -1067,24 +1078,18 @@ static int cells_to_planes(fvm2d_solver *s, const double *cells, int stride, voi
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(s->scratch, cells, bytes, kind, s->stream));
-    if (is_fp32(s->precision))
-        aos_to_soa<float><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, static_cast<float *>(dst), s->nx, s->ny,
-                                                          s->pitch, s->plane);
-    else
-        aos_to_soa<double><<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, static_cast<double *>(dst), s->nx,
-                                                           s->ny, s->pitch, s->plane);
+    with_planes(s->precision, dst, s->plane, [&](auto st) {
+        aos_to_soa<<<148 * 4, 256, 0, s->stream>>>(s->scratch, stride, st, s->nx, s->ny, s->pitch, s->plane);
+    });
     CK(cudaGetLastError());
     return FVM2D_OK;
 }
 
 static int planes_to_cells(fvm2d_solver *s, const void *src, double *cells, int stride)
 {
-    if (is_fp32(s->precision))
-        soa_to_aos<float><<<148 * 4, 256, 0, s->stream>>>(static_cast<const float *>(src), s->nx, s->ny, s->pitch,
-                                                          s->plane, stride, s->scratch);
-    else
-        soa_to_aos<double><<<148 * 4, 256, 0, s->stream>>>(static_cast<const double *>(src), s->nx, s->ny, s->pitch,
-                                                           s->plane, stride, s->scratch);
+    with_planes(s->precision, src, s->plane, [&](auto st) {
+        soa_to_aos<<<148 * 4, 256, 0, s->stream>>>(st, s->nx, s->ny, s->pitch, s->plane, stride, s->scratch);
+    });
     CK(cudaGetLastError());
     const size_t bytes = sizeof(double) * (size_t)s->nx * s->ny * stride;
     const cudaMemcpyKind kind = is_device_pointer(cells) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

@@ -84,6 +84,7 @@ FVM2D_DECLARE_VARIANT(fp64)
 FVM2D_DECLARE_VARIANT(fp64_strict)
 FVM2D_DECLARE_VARIANT(fp64_reforder)
 FVM2D_DECLARE_VARIANT(fp32)
+FVM2D_DECLARE_VARIANT(fp32r)
 FVM2D_DECLARE_VARIANT(jvp)
 
 // The FP64 and FP32 steps keeping what their adjoint needs: X(U) in c.A, Y(U)

@@ -25,8 +25,10 @@
 
 #include "fvm2d_control.h"
 #include "fvm2d_math.cuh"
+#include "fvm2d_split.cuh"
 
 #include <stdint.h>
+#include <type_traits>
 
 namespace fvm2d {
 namespace FVM2D_VARIANT {
@@ -204,11 +206,10 @@ __device__ __forceinline__ SweepConsts<Real> sweep_consts(const SweepArgs<Real> 
     K.h = Real(a.h);
     K.rh = Real(a.rh);
     K.alpha = Real(a.alpha);
-    K.g = Real(a.gamma);
+    set_gamma_consts(K, a.gamma);
     K.k = Real(dt);
     K.lambda = Real(dt / a.h);
-    K.igm1 = Real(1.0 / (a.gamma - 1.0));
-    K.kappa = Real((a.gamma + 1.0) / 2.0);
+    K.lambda_lo = Real(lo_part<Real>(dt / a.h));
     return K;
 }
 
@@ -230,6 +231,71 @@ __device__ __forceinline__ void store_cell(const Field<Real> &F, int x, int y, i
     F.at(1, x, y) = c.p;
     F.at(fn, x, y) = c.un;
     F.at(ft, x, y) = c.ut;
+}
+
+// ---- FP32 states with residual planes -------------------------------------
+// A stored value is the FP32 plane value plus its plane's 16-bit residual
+// (fvm2d_split.cuh).  With a physics that declares kSplitStorage (and
+// provides update_split), the sweeps read the FP32 values for slopes and
+// fluxes and hi + lo of the cell they update, and write the result split
+// again.
+template <class P, class = void>
+struct split_storage : std::false_type {};
+template <class P>
+struct split_storage<P, std::void_t<decltype(P::kSplitStorage)>> : std::integral_constant<bool, P::kSplitStorage> {};
+
+// the 8-byte word of a cell's 4 residuals (field f in bits 16 f .. 16 f + 15)
+template <typename Real>
+__device__ __forceinline__ unsigned long long &lo_cell(const Field<Real> &F, int x, int y)
+{
+    return reinterpret_cast<unsigned long long *>(residual_block(F.base, F.plane))[y * F.pitch + x];
+}
+
+// the residuals of a cell, as values of the arithmetic type
+template <typename Real>
+__device__ __forceinline__ Cell<Real> load_lo(const Field<Real> &F, int x, int y, int fn, int ft)
+{
+    const unsigned long long w = lo_cell(F, x, y);
+    auto part = [&](int f) { return Real(bf16_value((unsigned short)(w >> (16 * f)))); };
+    Cell<Real> c;
+    c.rho = part(0);
+    c.p = part(1);
+    c.un = part(fn);
+    c.ut = part(ft);
+    return c;
+}
+
+template <typename Real>
+__device__ __forceinline__ Cell<double> join_cell(const Cell<Real> &hi, const Cell<Real> &lo)
+{
+    return {double(hi.rho) + double(lo.rho), double(hi.p) + double(lo.p), double(hi.un) + double(lo.un),
+            double(hi.ut) + double(lo.ut)};
+}
+
+// v split into the FP32 planes and the cell's residual word; returns the
+// FP32 part
+template <typename Real>
+__device__ __forceinline__ Cell<Real> store_split(const Field<Real> &F, int x, int y, int fn, int ft,
+                                                  const Cell<double> &v)
+{
+    float h[4];
+    unsigned short l[4];
+    split_value(v.rho, h[0], l[0]);
+    split_value(v.p, h[1], l[1]);
+    split_value(v.un, h[2], l[fn]);
+    split_value(v.ut, h[3], l[ft]);
+    lo_cell(F, x, y) = (unsigned long long)l[0] | (unsigned long long)l[1] << 16 | (unsigned long long)l[2] << 32 |
+                       (unsigned long long)l[3] << 48;
+    const Cell<Real> hi = {Real(h[0]), Real(h[1]), Real(h[2]), Real(h[3])};
+    store_cell(F, x, y, fn, ft, hi);
+    return hi;
+}
+
+// a cell's residuals copied (ghost cells passing through a sweep)
+template <typename Real>
+__device__ __forceinline__ void copy_lo(const Field<Real> &from, const Field<Real> &to, int x, int y)
+{
+    lo_cell(to, x, y) = lo_cell(from, x, y);
 }
 
 // Value of the next (lane_down) or previous (lane_up) lane of the warp, or of
@@ -330,6 +396,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
     // a taped sweep (a.flux set) stores every interface flux; the same code
     // runs taped and untaped, so both give the same bits
     const bool tape = a.flux.base != nullptr;
+    constexpr bool kResidual = split_storage<Phys>::value;
     const int cells = x_item_cells(a.xchunks);
     const int b0 = 1 + seg * cells;
     const int last = min(b0 + cells, nx - 3);  // last cell this item updates
@@ -348,6 +415,21 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
             }
         } else {
             store_cell(a.dst, x, y, 2, 3, U);
+        }
+    };
+    // residual builds: U and Ab as hi + lo; the wave speed from the FP32 part
+    // as stored (as the init and ghost kernels see it)
+    auto emit_split = [&](int x, const Cell<double> &U, const Cell<double> &Ab) {
+        if (FINAL) {
+            const Cell<double> o = {(Ab.rho + U.rho) * 0.5, (Ab.p + U.p) * 0.5, (Ab.un + U.un) * 0.5,
+                                    (Ab.ut + U.ut) * 0.5};
+            const Cell<Real> h = store_split(a.dst, x, y, 2, 3, o);
+            if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3) {
+                vmax = fmax(vmax, wave_speed(h.rho, h.p, h.un, h.ut, a.gamma));
+                bad |= !(h.rho > Real(0) && h.p > Real(0));
+            }
+        } else {
+            store_split(a.dst, x, y, 2, 3, U);
         }
     };
     // chunk m's cell of this lane into its ring slot
@@ -397,8 +479,9 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
             c0 = ld(c);
             cp1 = ld(c + 1);
         }
-        Cell<Real> A;
+        Cell<Real> A, Alo;
         if (FINAL) A = load_cell(a.comb, min(max(u, 0), nx - 1), y, 2, 3);  // branch A, loaded early
+        if (FINAL && kResidual) Alo = load_lo(a.comb, min(max(u, 0), nx - 1), y, 2, 3);
         const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);                // slope of cell c
         Cell<Real> sm1 = shfl_up(s0);                                     // slope of cell c-1
         if (lane == 0) sm1 = cs;
@@ -407,7 +490,12 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
         if (tape && (j > 0 || lane >= 1) && c <= nx - 2) store_cell(a.flux, c, y, 2, 3, F);  // at cell c
         Cell<Real> FL = shfl_up(F);                                       // interface c-3/2
         if (lane == 0) FL = cF;
-        if ((j > 0 || lane >= 2) && u <= last) emit(u, Phys::update(cm1, FL, F, K), A);
+        if ((j > 0 || lane >= 2) && u <= last) {
+            if constexpr (kResidual)
+                emit_split(u, Phys::update_split(cm1, load_lo(a.src, u, y, 2, 3), FL, F, K), join_cell(A, Alo));
+            else
+                emit(u, Phys::update(cm1, FL, F, K), A);
+        }
         cs = shfl_last(s0);
         cF = shfl_last(F);
     }
@@ -416,16 +504,20 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
         __syncwarp();
     }
     // ghost columns pass through (x-sweeps do not update them, src/basicFuns.cuh:235)
-    if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
-        const int x = seg == 0 ? lane : nx - 2 + lane;
+    auto pass = [&](int x) {
         Cell<Real> Ab;
         if (FINAL) Ab = load_cell(a.comb, x, y, 2, 3);
-        emit(x, ld(x), Ab);
-        if (seg == 0 && seg == nseg - 1) {
-            const int x2 = nx - 2 + lane;
-            if (FINAL) Ab = load_cell(a.comb, x2, y, 2, 3);
-            emit(x2, ld(x2), Ab);
+        if constexpr (kResidual) {
+            Cell<Real> Ablo;
+            if (FINAL) Ablo = load_lo(a.comb, x, y, 2, 3);
+            emit_split(x, join_cell(ld(x), load_lo(a.src, x, y, 2, 3)), join_cell(Ab, Ablo));
+        } else {
+            emit(x, ld(x), Ab);
         }
+    };
+    if (lane < 2 && (seg == 0 || seg == nseg - 1)) {
+        pass(seg == 0 ? lane : nx - 2 + lane);
+        if (seg == 0 && seg == nseg - 1) pass(nx - 2 + lane);
     }
 }
 
@@ -482,6 +574,7 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
 {
     const int nx = a.nx, ny = a.ny;
     const bool tape = a.flux.base != nullptr;  // as in x_item
+    constexpr bool kResidual = split_storage<Phys>::value;
     const int x = cw * 32 + lane;
     const bool col = x < nx;
     const int xc = col ? x : nx - 1;
@@ -497,7 +590,12 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
             const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
             const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
             if (tape && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);  // interface l-1/2 at line position l
-            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));  // cell l-1
+            if (l > l0 && col) {  // cell l-1
+                if constexpr (kResidual)
+                    store_split(a.dst, x, ny - l, 3, 2, Phys::update_split(cm1, load_lo(a.src, x, ny - l, 3, 2), Fp, F, K));
+                else
+                    store_cell(a.dst, x, ny - l, 3, 2, Phys::update(cm1, Fp, F, K));
+            }
             Fp = F;
             cm1 = c0;
             c0 = cp1;
@@ -541,17 +639,26 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
             const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);
             const Cell<Real> F = Phys::interface_flux(cm1, c0, sm1, s0, K);
             if (tape && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);
-            if (l > l0 && col) store_cell(a.dst, x, ny - l, 3, 2, Phys::update(get(l - 1), Fp, F, K));
+            if (l > l0 && col) {
+                if constexpr (kResidual)
+                    store_split(a.dst, x, ny - l, 3, 2, Phys::update_split(cm1, load_lo(a.src, x, ny - l, 3, 2), Fp, F, K));
+                else
+                    store_cell(a.dst, x, ny - l, 3, 2, Phys::update(get(l - 1), Fp, F, K));
+            }
             Fp = F;
             sm1 = s0;
         }
         async_wait<0>();  // no copy of this item may land in the ring after it
     }
     // ghost rows pass through (y-sweeps do not update them)
+    auto pass = [&](int l) {
+        store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+        if constexpr (kResidual) copy_lo(a.src, a.dst, x, ny - 1 - l);
+    };
     if (col && seg == 0)
-        for (int l = 0; l < 2; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+        for (int l = 0; l < 2; ++l) pass(l);
     if (col && seg == nseg - 1)
-        for (int l = ny - 2; l < ny; ++l) store_cell(a.dst, x, ny - 1 - l, 3, 2, ld(l));
+        for (int l = ny - 2; l < ny; ++l) pass(l);
 }
 
 // prefetch distance of the y walker's shared-memory ring (rows; 0: no ring);
@@ -607,6 +714,7 @@ struct GhostArgs {
     PlanParams plan;
     int row0, gny;               // global row of local row 0; global row count
     int fill_top, fill_bottom;   // 0: that pair of ring rows is a halo (not filled, no max)
+    int residual = 0;            // 1: the state has residual planes (a ring cell's are zeroed)
 };
 
 template <typename Real>
@@ -730,6 +838,7 @@ __device__ __forceinline__ double ghost_cell(const GhostArgs<Real> &a, int k, do
     a.U.at(1, i, j) = c.p;
     a.U.at(2, i, j) = c.un;
     a.U.at(3, i, j) = c.ut;
+    if (a.residual) lo_cell(a.U, i, j) = 0ull;  // a ring cell holds its FP32 value exactly
     return wave_speed(c.rho, c.p, c.un, c.ut, a.gamma);
 }
 

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
+#include <type_traits>
 
 #ifndef FVM2D_VARIANT
 #error "define FVM2D_VARIANT (the namespace of this build of the kernels) first"
@@ -292,7 +293,37 @@ struct SweepConsts {
     Real h, rh, alpha, g;  // spacing, 1/h, limiter parameter, gamma
     Real k, lambda;        // dt and dt/h
     Real igm1, kappa;      // 1/(gamma-1), (gamma+1)/2   (Hoisted only)
+    // 1/(gamma-1) and gamma-1 as hi + lo pairs of the arithmetic type (lo = 0
+    // unless Real is float), for the compensated FP32 update: it converts p
+    // to E and back once per sweep, and with the rounded constants alone
+    // (2.5f and 1.4f - 1 for gamma 1.4) every round trip scales the internal
+    // energy by 1 - 6e-8, a bias that grows with the number of sweeps
+    Real igm1_lo, gm1, gm1_lo;
+    Real lambda_lo;  // dt/h - lambda (0 unless Real is float): the FP64 update of residual builds
 };
+
+// The part of x that Real does not hold: 0 unless Real is float.
+template <typename Real>
+__host__ __device__ inline double lo_part(double x)
+{
+    if constexpr (std::is_same<Real, float>::value)
+        return x - double(float(x));
+    else
+        return 0.0;
+}
+
+// The constants of gamma in SweepConsts.
+template <typename Real>
+__host__ __device__ inline void set_gamma_consts(SweepConsts<Real> &K, double gamma)
+{
+    const double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
+    K.g = Real(gamma);
+    K.igm1 = Real(igm1);
+    K.igm1_lo = Real(lo_part<Real>(igm1));
+    K.gm1 = Real(gm1);
+    K.gm1_lo = Real(lo_part<Real>(gm1));
+    K.kappa = Real((gamma + 1.0) / 2.0);
+}
 
 template <typename Real>
 __device__ __forceinline__ Cell<Real> cell_slope(const Cell<Real> &m, const Cell<Real> &c, const Cell<Real> &p,
@@ -576,6 +607,7 @@ struct HoistedCompensated : Hoisted {
         kine += kae + kbe + m1e * U.un + m3e * U.ut;  // rho (un^2 + ut^2) = kin + kine
         Real pe, pee, E, Ee;
         two_prod(U.p, K.igm1, pe, pee);
+        pee = fma(U.p, K.igm1_lo, pee);  // p / (gamma - 1) = pe + pee
         two_sum(pe, half * kin, E, Ee);
         Ee += pee + half * kine;
         // W - lambda (F_R - F_L), compensated
@@ -601,7 +633,8 @@ struct HoistedCompensated : Hoisted {
         k2e += kue + kve + e1 * o.un + e3 * o.ut;  // m . u = k2 + k2e
         Real d, de;
         two_sum(s2, -half * k2, d, de);
-        o.p = (K.g - Real(1)) * (d + (de + e2 - half * k2e));
+        const Real ei = d + (de + e2 - half * k2e);  // internal energy
+        o.p = fma(K.gm1, ei, K.gm1_lo * ei);        // (gamma - 1) ei with the constant's low part
         return o;
     }
 };

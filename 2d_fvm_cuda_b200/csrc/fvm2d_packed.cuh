@@ -70,6 +70,7 @@ struct PackedCompensated : HoistedCompensated {
         kine += kt.x + kt.y;  // rho (un^2 + ut^2) = kin + kine
         float pe, pee, E, Ee;
         two_prod(U.p, K.igm1, pe, pee);
+        pee = fmaf(U.p, K.igm1_lo, pee);  // p / (gamma - 1) = pe + pee
         two_sum(pe, 0.5f * kin, E, Ee);
         Ee += pee + 0.5f * kine;
         // W - lambda (F_R - F_L) on the pairs (rho, m1) and (E, m3)
@@ -98,7 +99,42 @@ struct PackedCompensated : HoistedCompensated {
         k2e += kt2.x + kt2.y;  // m . u = k2 + k2e
         float d, de;
         two_sum(s23.x, -0.5f * k2, d, de);
-        o.p = (K.g - 1.0f) * (d + (de + e2 - 0.5f * k2e));
+        const float ei = d + (de + e2 - 0.5f * k2e);  // internal energy
+        o.p = fmaf(K.gm1, ei, K.gm1_lo * ei);        // (gamma - 1) ei with the constant's low part
+        return o;
+    }
+};
+
+// The FP32 physics of the build with residual planes (FVM2D_FP32_RESIDUAL):
+// slopes and fluxes from the FP32 values as PackedCompensated computes them;
+// the conservative update of a cell from its stored hi + lo in FP64, with
+// dt/h, 1/(gamma-1) and gamma-1 as hi + lo pairs, the result returned
+// unrounded for the caller to split into the two planes.  (An FP64 update
+// costs fewer instructions than the compensated FP32 one, and the FP64 pipe
+// is otherwise idle in these sweeps.)
+struct PackedResidual : PackedCompensated {
+    static constexpr bool kSplitStorage = true;
+    __device__ static __forceinline__ Cell<double> update_split(const Cell<float> &U, const Cell<float> &L,
+                                                                const Cell<float> &FL, const Cell<float> &FR,
+                                                                const SweepConsts<float> &K)
+    {
+        const double rho = double(U.rho) + double(L.rho), p = double(U.p) + double(L.p);
+        const double un = double(U.un) + double(L.un), ut = double(U.ut) + double(L.ut);
+        const double lam = double(K.lambda) + double(K.lambda_lo);
+        const double igm1 = double(K.igm1) + double(K.igm1_lo), gm1 = double(K.gm1) + double(K.gm1_lo);
+        double m0 = rho, m1 = rho * un, m3 = rho * ut;
+        double m2 = fma(p, igm1, 0.5 * (m1 * un + m3 * ut));
+        // W - lambda (F_R - F_L); the flux differences are exact in FP64
+        m0 = fma(double(FL.rho) - double(FR.rho), lam, m0);
+        m1 = fma(double(FL.p) - double(FR.p), lam, m1);
+        m2 = fma(double(FL.un) - double(FR.un), lam, m2);
+        m3 = fma(double(FL.ut) - double(FR.ut), lam, m3);
+        const double ir = rrcp(m0);
+        Cell<double> o;
+        o.rho = m0;
+        o.un = m1 * ir;
+        o.ut = m3 * ir;
+        o.p = gm1 * (m2 - 0.5 * (m1 * o.un + m3 * o.ut));
         return o;
     }
 };

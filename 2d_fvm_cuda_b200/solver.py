@@ -30,6 +30,7 @@ class precision(enum.IntEnum):
     fp64_strict = _lib.FP64_STRICT      # reference order, no contraction: bit-exact with the reference -fmad=false
     fp64_reforder = _lib.FP64_REFORDER  # reference order with FMA contraction, as the reference's own build
     fp32 = _lib.FP32                    # FP32 storage/arithmetic, compensated update, FP64 dt
+    fp32_residual = _lib.FP32_RESIDUAL  # FP32 arithmetic, FP32 + 16-bit residual planes, FP64 update
 
 
 def write_matrix_txt(dir: str, U, t: float) -> None:

@@ -196,9 +196,9 @@ def product_arm(args, rank, world, local_rank):
     pkg = importlib.import_module("2d_fvm_cuda_b200")
     n = args.n
     U0 = pkg.scenarios.seeded_four_quadrant(n, n, rank)
-    prec = pkg.FP32 if args.precision == "fp32" else pkg.FP64
+    prec = {"fp32": pkg.FP32, "fp32r": pkg.FP32_RESIDUAL}.get(args.precision, pkg.FP64)
     if prec != pkg.FP64 and not args.kernels_only:
-        raise SystemExit("--precision fp32 applies to --kernels-only runs; the full line reports FP32 beside FP64")
+        raise SystemExit("--precision fp32/fp32r applies to --kernels-only runs; the full line reports them beside FP64")
     # the clock sampler starts first, so it is recording by the time the
     # steps run (the timed region lasts tens of milliseconds, less than its
     # 100 ms period): samples come from the warm-up, the timed steps and the
@@ -231,7 +231,7 @@ def product_arm(args, rank, world, local_rank):
 
     # per-kernel CUDA-event durations (steps run one at a time, outside the graph);
     # the dominant kernel is the one with the largest share of a step
-    kernel_ms, kp = h.profile_kernels(5)
+    kernel_ms, _ = h.profile_kernels(5)
     groups = {"sweep_x": [0], "sweep_y": [1, 2], "sweep_x_final": [3], "ghost_fill": [4]}
     alg_bytes = {"sweep_x": 64 * n * n, "sweep_y": 64 * n * n, "sweep_x_final": 96 * n * n,
                  "ghost_fill": 64 * (4 * n + 4 * (n - 4))}
@@ -260,36 +260,47 @@ def product_arm(args, rank, world, local_rank):
             fp64_pipe = {"flops_per_cell": per_cell, "achieved_tflops": ach_tf, "peak_tflops": peak_tf,
                          "peak_kind": "measured (fvm2d_measure_fp64_peak)", "frac": ach_tf / peak_tf}
 
+    # the steps the FP64 handle has run: warm-up, clock-sampling (a variable
+    # number of 8-step runs), timed and profiled steps; the comparison runs
+    # below run as many
+    steps_run = h.time()[1]
     # L1 difference of the FMA product from the contraction-free build on the same steps
     hs = pkg.Handle(n, n)
     hs.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
                  CFG["strategy"], pkg.FP64_STRICT)
     hs.set_state(U0)
-    hs.advance(args.warmup + 8 + args.steps + kp)
+    hs.advance(steps_run)
     A, B = h.get_state(4), hs.get_state(4)
     l1 = [float(np.abs(A[..., f] - B[..., f]).sum() / np.abs(B[..., f]).sum()) for f in range(4)]
     hs.close()
 
-    # FP32 form on the same workload and steps: speed and density error vs FP64
-    hf = pkg.Handle(n, n)
-    hf.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
-                 CFG["strategy"], pkg.FP32)
-    hf.set_state(U0)
-    hf.advance(args.warmup + 8)
-    hf.advance(args.steps)
-    f32_ms, _ = hf.run_stats()
-    hf.advance(kp)
-    F32 = hf.get_state(4)
-    f32_l1 = [float(np.abs(F32[..., f] - A[..., f]).sum() / np.abs(A[..., f]).sum()) for f in range(4)]
-    f32_linf = [float(np.abs(F32[..., f] - A[..., f]).max()) for f in range(4)]
-    hf.close()
-    f32_ms = allreduce_max(dist, f32_ms)
-    fp32 = {"value": n * n * args.steps * world / (f32_ms / 1e3), "unit": UNIT, "ms_per_step": f32_ms / args.steps,
-            "speedup_vs_fp64": dev_ms_max / f32_ms,
-            "l1_rel_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_l1,
-                               "steps": args.warmup + 8 + args.steps + kp},
-            "linf_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_linf},
-            "arithmetic": "FP32 planes and arithmetic, compensated update, FP64 wave-speed max and dt"}
+    # FP32 forms on the same workload and steps: speed and density error vs FP64
+    def single_precision(prec, arithmetic):
+        hf = pkg.Handle(n, n)
+        hf.configure(CFG["width"], CFG["height"], CFG["t_end"], CFG["cfl"], CFG["alpha"], CFG["gamma"],
+                     CFG["strategy"], prec)
+        hf.set_state(U0)
+        hf.advance(args.warmup + 8)
+        hf.advance(args.steps)
+        f32_ms, _ = hf.run_stats()
+        hf.advance(steps_run - (args.warmup + 8 + args.steps))
+        assert hf.time()[1] == steps_run
+        F32 = hf.get_state(4)
+        f32_l1 = [float(np.abs(F32[..., f] - A[..., f]).sum() / np.abs(A[..., f]).sum()) for f in range(4)]
+        f32_linf = [float(np.abs(F32[..., f] - A[..., f]).max()) for f in range(4)]
+        hf.close()
+        f32_ms = allreduce_max(dist, f32_ms)
+        return {"value": n * n * args.steps * world / (f32_ms / 1e3), "unit": UNIT,
+                "ms_per_step": f32_ms / args.steps, "speedup_vs_fp64": dev_ms_max / f32_ms,
+                "l1_rel_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_l1,
+                                   "steps": steps_run},
+                "linf_vs_fp64": {"fields": ["rho", "p", "u", "v"], "value": f32_linf},
+                "arithmetic": arithmetic}
+
+    fp32 = single_precision(pkg.FP32, "FP32 planes and arithmetic, compensated update, FP64 wave-speed max and dt")
+    fp32["residual"] = single_precision(
+        pkg.FP32_RESIDUAL, "FP32 slopes and fluxes; FP32 planes + 16-bit residual planes; the update in FP64 on "
+                           "hi + lo; FP64 wave-speed max and dt")
 
     # e2e through the C ABI with pinned host buffers
     import torch
@@ -361,7 +372,7 @@ def product_arm(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}"},
             "l1_rel_vs_reference_order": {"fields": ["rho", "p", "u", "v"], "value": l1,
                                           "against": "contraction-free build, bit-exact with the reference -fmad=false",
-                                          "steps": args.warmup + 8 + args.steps + kp},
+                                          "steps": steps_run},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": 64 + state_bytes / args.steps,
                     "path": "fvm2d_set_state(pinned) + steps x fvm2d_advance(1) + fvm2d_get_state(pinned)"},
@@ -758,7 +769,7 @@ def form_vortex(args, with_reference_order=False):
     U0 = sc.isentropic_vortex(n)
     res = {}
     states = {}
-    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32")):
+    for prec, name in ((pkg.FP64, "fp64"), (pkg.FP32, "fp32"), (pkg.FP32_RESIDUAL, "fp32_residual")):
         h = pkg.Handle(n, n)
         h.configure(w, hgt, 10.0, 0.45, 1.9, 1.4, 5, prec)
         h.set_state(U0)
@@ -775,11 +786,13 @@ def form_vortex(args, with_reference_order=False):
         return float(np.abs(A[inner][..., 0] - B[inner][..., 0]).sum() / np.abs(B[inner][..., 0]).sum())
 
     res["fp64"]["rho_rel_l1_vs_exact"] = rl1(states["fp64"], E)
-    res["fp32"]["rho_rel_l1_vs_exact"] = rl1(states["fp32"], E)
-    res["fp32"]["rho_rel_l1_vs_fp64"] = rl1(states["fp32"], states["fp64"])
-    res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(states["fp32"][inner][..., 0] - states["fp64"][inner][..., 0]).max())
-    res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
-    res["fp32"]["rho_rel_l1_target"] = 1e-5
+    for name in ("fp32", "fp32_residual"):
+        res[name]["rho_rel_l1_vs_exact"] = rl1(states[name], E)
+        res[name]["rho_rel_l1_vs_fp64"] = rl1(states[name], states["fp64"])
+        res[name]["rho_linf_vs_fp64"] = float(np.abs(states[name][inner][..., 0] -
+                                                     states["fp64"][inner][..., 0]).max())
+        res[name]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res[name]["device_s"]
+        res[name]["rho_rel_l1_target"] = 1e-5
     return {"form": "vortex", "workload": "2000^2 periodic isentropic vortex, one period", "results": res,
             "preset_parity": "periodic is not a reference preset: its ghost rule is pinned to the oracle's "
                              "restatement only"}
@@ -800,7 +813,7 @@ def form_precision(args, with_reference_order=True):
     # FP64_REFORDER (the reference's operation order) differs from FP64 by
     # rounding only: how far two FP64 runs drift apart on this flow (five
     # times slower than FP64, so left out of the default bench line)
-    builds = [(pkg.FP64, "fp64"), (pkg.FP32, "fp32")]
+    builds = [(pkg.FP64, "fp64"), (pkg.FP32, "fp32"), (pkg.FP32_RESIDUAL, "fp32_residual")]
     if with_reference_order:
         builds.append((pkg.FP64_REFORDER, "fp64_reference_order"))
     for prec, name in builds:
@@ -813,11 +826,13 @@ def form_precision(args, with_reference_order=True):
         states[name] = h.get_state(4)[..., 0]
         h.close()
         res[name] = {"steps": steps, "t": t, "device_s": ms / 1e3, "cell_updates_per_s": n * n * steps / (ms / 1e3)}
-    D, S = states["fp64"], states["fp32"]
-    res["fp32"]["rho_rel_l1_vs_fp64"] = float(np.abs(S - D).sum() / np.abs(D).sum())
-    res["fp32"]["rho_linf_vs_fp64"] = float(np.abs(S - D).max())
-    res["fp32"]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res["fp32"]["device_s"]
-    res["fp32"]["rho_rel_l1_target"] = 1e-5
+    D = states["fp64"]
+    for name in ("fp32", "fp32_residual"):
+        S = states[name]
+        res[name]["rho_rel_l1_vs_fp64"] = float(np.abs(S - D).sum() / np.abs(D).sum())
+        res[name]["rho_linf_vs_fp64"] = float(np.abs(S - D).max())
+        res[name]["speedup_vs_fp64"] = res["fp64"]["device_s"] / res[name]["device_s"]
+        res[name]["rho_rel_l1_target"] = 1e-5
     if with_reference_order:
         Rf = states["fp64_reference_order"]
         res["fp64_reference_order"]["rho_rel_l1_vs_fp64"] = float(np.abs(Rf - D).sum() / np.abs(D).sum())
@@ -836,7 +851,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side incl. ghosts (profiling cases)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device-resident steps only (profiling cases; no e2e or baselines)")
-    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+    ap.add_argument("--precision", choices=["fp64", "fp32", "fp32r"], default="fp64",
                     help="arithmetic of a --kernels-only run")
     ap.add_argument("--slabs", action="store_true",
                     help="the row-slab path (the default for N > 1) also on one GPU, under torchrun")

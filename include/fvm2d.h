@@ -58,9 +58,14 @@ enum fvm2d_precision {
                                 with the reference built -fmad=false */
     FVM2D_FP64_REFORDER = 2, /* FP64, the reference's operation order with FMA contraction, as the
                                 reference's own (default) build computes */
-    FVM2D_FP32 = 3           /* FP32 state planes and arithmetic with a compensated conservative
+    FVM2D_FP32 = 3,          /* FP32 state planes and arithmetic with a compensated conservative
                                 update; wave-speed max, dt and time stay FP64.  Host-side states
                                 remain doubles (converted on upload and download). */
+    FVM2D_FP32_RESIDUAL = 4  /* FP32 slopes and fluxes; each stored value is an FP32 plane value
+                                plus a 16-bit (bfloat16) residual plane value, about 32
+                                significant bits in 6 bytes, and the conservative update runs
+                                in FP64 on hi + lo.  Solver handles only (no batches, no
+                                differentiation). */
 };
 
 typedef struct fvm2d_solver fvm2d_solver;

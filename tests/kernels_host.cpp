@@ -358,36 +358,43 @@ int kh_batch_solve(int np, const int *nx, const int *ny, const double *params, c
     return 0;
 }
 
-// A solve through the single-problem kernels in the reference order
-// (RefOrder), launched as a solver's step graphs launch them: init_kernel,
-// then per step sweep_x_kernel, sweep_y_kernel twice, the final
-// sweep_x_kernel and ghost_kernel, on `blocks` blocks of 128 threads per
-// sweep (grid-stride), until the control record ends the loop or max_steps.
-// out: final state; t, steps and the health record's first bad step.
-int kh_solve(const double *cells, int nx, int ny, double width, double height, double t_end, double cfl,
-             double alpha, double gamma, int strategy, int T, int blocks, int max_steps, double *out, double *t,
-             int *steps, int *first_bad)
+} // extern "C"
+
+// The body of kh_solve for a storage type R and physics Phys; SPLIT: the
+// states hold residual planes after the FP32 planes (fvm2d_split.cuh).
+template <typename R, class Phys, bool SPLIT>
+static int solve_impl(const double *cells, int nx, int ny, double width, double height, double t_end, double cfl,
+                      double alpha, double gamma, int strategy, int T, int blocks, int max_steps, double *out,
+                      double *t, int *steps, int *first_bad)
 {
     constexpr int kNT = 128, kGhostNT = 256, kInitNT = 256;
     if (nx < 6 || ny < 6 || blocks < 1) return 1;
     const int pitch = (nx + 31) / 32 * 32;
     const long long plane = (long long)pitch * ny;
-    std::vector<double> Uv(4 * plane, 0.0), Av(4 * plane, 0.0), Bv(4 * plane, 0.0);
+    const long long per_state = (SPLIT ? 6 : 4) * plane;  // 4 FP32 planes + 4 planes of 16-bit residuals
+    std::vector<R> Uv(per_state, R(0.0)), Av(per_state, R(0.0)), Bv(per_state, R(0.0));
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x)
-            for (int f = 0; f < 4; ++f) Uv[f * plane + (long long)y * pitch + x] = cells[4 * ((long long)y * nx + x) + f];
-    const Field<double> U{Uv.data(), plane, pitch}, A{Av.data(), plane, pitch}, B{Bv.data(), plane, pitch};
+            for (int f = 0; f < 4; ++f) {
+                const long long k = f * plane + (long long)y * pitch + x;
+                const double v = cells[4 * ((long long)y * nx + x) + f];
+                if constexpr (SPLIT)
+                    fvm2d::split_planes(Uv.data(), plane).put(k, v);
+                else
+                    Uv[k] = R(v);
+            }
+    const Field<R> U{Uv.data(), plane, pitch}, A{Av.data(), plane, pitch}, B{Bv.data(), plane, pitch};
     StepControl ctl;
     std::memset(&ctl, 0, sizeof ctl);
     ctl.step_limit = max_steps;
     const double hx = width / nx, hy = height / ny;
     const PlanParams plan{t_end, cfl, hy < hx ? hy : hx, 0.0};
-    auto args = [&](const Field<double> &src, const Field<double> &dst, int dir) {
-        SweepArgs<double> a;
+    auto args = [&](const Field<R> &src, const Field<R> &dst, int dir) {
+        SweepArgs<R> a;
         a.src = src;
         a.dst = dst;
         a.comb = dst;
-        a.flux = Field<double>{nullptr, plane, pitch};
+        a.flux = Field<R>{nullptr, plane, pitch};
         a.xchunks = g_xchunks;
         a.nx = nx;
         a.ny = ny;
@@ -398,7 +405,7 @@ int kh_solve(const double *cells, int nx, int ny, double width, double height, d
         a.ctl = &ctl;
         return a;
     };
-    GhostArgs<double> g;
+    GhostArgs<R> g;
     g.U = U;
     g.nx = nx;
     g.ny = ny;
@@ -409,24 +416,67 @@ int kh_solve(const double *cells, int nx, int ny, double width, double height, d
     g.row0 = 0;
     g.gny = ny;
     g.fill_top = g.fill_bottom = 1;
+    g.residual = SPLIT;
     const int ring = 4 * nx + 4 * (ny - 4);
-    emu::launch(dim3(2), dim3(kInitNT), true, [&] { init_kernel<double, kInitNT>(U, nx, ny, gamma, &ctl, plan); });
+    emu::launch(dim3(2), dim3(kInitNT), true, [&] { init_kernel<R, kInitNT>(U, nx, ny, gamma, &ctl, plan); });
     for (int k = 0; k < max_steps && ctl.active; ++k) {
-        const SweepArgs<double> ax = args(U, A, 0), ay = args(U, B, 1), aya = args(A, U, 1), axf = args(B, U, 0);
-        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<double, RefOrder, false, kNT, 1>(ax); });
-        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<double, RefOrder, kNT, 1>(ay, T); });
-        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<double, RefOrder, kNT, 1>(aya, T); });
-        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<double, RefOrder, true, kNT, 1>(axf); });
+        const SweepArgs<R> ax = args(U, A, 0), ay = args(U, B, 1), aya = args(A, U, 1), axf = args(B, U, 0);
+        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<R, Phys, false, kNT, 1>(ax); });
+        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<R, Phys, kNT, 1>(ay, T); });
+        emu::launch(dim3(blocks), dim3(kNT), false, [&] { sweep_y_kernel<R, Phys, kNT, 1>(aya, T); });
+        emu::launch(dim3(blocks), dim3(kNT), true, [&] { sweep_x_kernel<R, Phys, true, kNT, 1>(axf); });
         emu::launch(dim3((ring + kGhostNT - 1) / kGhostNT), dim3(kGhostNT), true,
-                    [&] { ghost_kernel<double, kGhostNT>(g); });
+                    [&] { ghost_kernel<R, kGhostNT>(g); });
     }
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x)
-            for (int f = 0; f < 4; ++f) out[4 * ((long long)y * nx + x) + f] = Uv[f * plane + (long long)y * pitch + x];
+            for (int f = 0; f < 4; ++f) {
+                const long long k = f * plane + (long long)y * pitch + x;
+                double v;
+                if constexpr (SPLIT)
+                    v = fvm2d::split_planes(Uv.data(), plane).get(k);
+                else
+                    v = double(Uv[k]);
+                out[4 * ((long long)y * nx + x) + f] = v;
+            }
     *t = ctl.t;
     *steps = ctl.steps;
     *first_bad = ctl.first_bad;
     return 0;
+}
+
+extern "C" {
+
+// A solve through the single-problem kernels in the reference order
+// (RefOrder), launched as a solver's step graphs launch them: init_kernel,
+// then per step sweep_x_kernel, sweep_y_kernel twice, the final
+// sweep_x_kernel and ghost_kernel, on `blocks` blocks of 128 threads per
+// sweep (grid-stride), until the control record ends the loop or max_steps.
+// out: final state; t, steps and the health record's first bad step.
+int kh_solve(const double *cells, int nx, int ny, double width, double height, double t_end, double cfl,
+             double alpha, double gamma, int strategy, int T, int blocks, int max_steps, double *out, double *t,
+             int *steps, int *first_bad)
+{
+    return solve_impl<double, RefOrder, false>(cells, nx, ny, width, height, t_end, cfl, alpha, gamma, strategy, T,
+                                               blocks, max_steps, out, t, steps, first_bad);
+}
+
+// kh_solve through the builds' own physics: 0 the FP64 default (Hoisted),
+// 1 FP32 (PackedCompensated), 2 FP32 with residual planes (PackedResidual).
+int kh_solve_build(int build, const double *cells, int nx, int ny, double width, double height, double t_end,
+                   double cfl, double alpha, double gamma, int strategy, int T, int blocks, int max_steps, double *out,
+                   double *t, int *steps, int *first_bad)
+{
+    if (build == 0)
+        return solve_impl<double, Hoisted, false>(cells, nx, ny, width, height, t_end, cfl, alpha, gamma, strategy, T,
+                                                  blocks, max_steps, out, t, steps, first_bad);
+    if (build == 1)
+        return solve_impl<float, PackedCompensated, false>(cells, nx, ny, width, height, t_end, cfl, alpha, gamma,
+                                                           strategy, T, blocks, max_steps, out, t, steps, first_bad);
+    if (build == 2)
+        return solve_impl<float, PackedResidual, true>(cells, nx, ny, width, height, t_end, cfl, alpha, gamma,
+                                                       strategy, T, blocks, max_steps, out, t, steps, first_bad);
+    return 1;
 }
 
 // A frame of a (ny, nx, 4) state as a solver writes one: the density range

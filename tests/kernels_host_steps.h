@@ -113,11 +113,10 @@ SweepConsts<A> adjoint_consts(double h, double dt, double alpha, double gamma)
     K.h = h;
     K.rh = 1.0 / h;
     K.alpha = alpha;
-    K.g = gamma;
+    set_gamma_consts(K, gamma);
     K.k = dt;
     K.lambda = dt / h;
-    K.igm1 = 1.0 / (gamma - 1.0);
-    K.kappa = (gamma + 1.0) / 2.0;
+    K.lambda_lo = 0.0;
     return K;
 }
 

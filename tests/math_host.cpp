@@ -44,6 +44,7 @@ static inline T __shfl_sync(unsigned, T v, int) { return v; }
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_adjoint_math.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_dual.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_split.cuh"
 
 // A number that counts the operations done on it, to state how many
 // divisions and square roots each policy spends per interface.
@@ -109,11 +110,10 @@ SweepConsts<Real> consts(const double *k4)
     K.h = Real(h);
     K.rh = Real(1.0 / h);
     K.alpha = Real(alpha);
-    K.g = Real(g);
+    set_gamma_consts(K, g);
     K.k = Real(k);
     K.lambda = Real(k / h);
-    K.igm1 = Real(1.0 / (g - 1.0));
-    K.kappa = Real((g + 1.0) / 2.0);
+    K.lambda_lo = Real(lo_part<Real>(k / h));
     return K;
 }
 
@@ -361,6 +361,23 @@ int mh_slope_vjp(long n, const double *in, const double *w, const double *k4, do
 // multiplications, divisions (by a variable), divisions by the constant 2,
 // square roots, reciprocal square roots, fused multiply-adds, comparisons.  Constant operands formed once per sweep
 // (SweepConsts) are not counted.
+// The residual storage's split of each x (fvm2d_split.cuh): out[3k] = hi,
+// out[3k+1] = the residual's value, out[3k+2] = 1 when splitting hi + lo
+// again gives the same hi and lo bits.
+int mh_split(long n, const double *x, double *out)
+{
+    for (long k = 0; k < n; ++k) {
+        float hi, hi2;
+        unsigned short lo, lo2;
+        fvm2d::split_value(x[k], hi, lo);
+        fvm2d::split_value(fvm2d::join_value(hi, lo), hi2, lo2);
+        out[3 * k] = hi;
+        out[3 * k + 1] = fvm2d::bf16_value(lo);
+        out[3 * k + 2] = (memcmp(&hi, &hi2, 4) == 0 && lo == lo2) ? 1.0 : 0.0;
+    }
+    return 0;
+}
+
 int mh_count(int policy, int what, const double *in, const double *k4, long *counts)
 {
     using opcount::Num;

@@ -82,6 +82,8 @@ def _kernels_host(tmp_path_factory, defines=()):
     lib.kh_sweep.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_solve.argtypes = ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 +
                              [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4)
+    lib.kh_solve_build.argtypes = ([ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 +
+                                   [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4)
     lib.kh_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
     lib.kh_batch_solve.argtypes = ([ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4 +
                                    [ctypes.c_void_p] * 3)
@@ -382,6 +384,19 @@ def kernel_solve(kh, U, kw, blocks, max_steps, T=16):
     return out, steps.value, t.value, bad.value
 
 
+def build_solve(kh, build, U, kw, blocks, max_steps, T=16):
+    """kh_solve through a build's physics: 0 FP64 (Hoisted), 1 FP32, 2 FP32
+    with residual planes."""
+    U = np.ascontiguousarray(U[..., :4], dtype=np.float64)
+    ny, nx = U.shape[:2]
+    out = np.empty_like(U)
+    t, steps, bad = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    assert kh.kh_solve_build(build, U.ctypes.data, nx, ny, kw["width"], kw["height"], kw["t_end"], kw["cfl"],
+                             kw["alpha"], kw["gamma"], kw["strategy"], T, blocks, max_steps, out.ctypes.data,
+                             ctypes.byref(t), ctypes.byref(steps), ctypes.byref(bad)) == 0
+    return out, steps.value, t.value, bad.value
+
+
 @pytest.mark.parametrize("strategy", range(7))
 def test_single_problem_kernels_solve_like_the_oracle(kh, oracle, pkg, strategy):
     """init_kernel, then the five kernels of a step as the step graphs launch
@@ -398,6 +413,36 @@ def test_single_problem_kernels_solve_like_the_oracle(kh, oracle, pkg, strategy)
         V, steps, t, bad = kernel_solve(kh, U, kw, blocks, 15)
         assert (steps, t, bad) == (rsteps, rt, 0), blocks
         assert np.array_equal(V, R, equal_nan=True), blocks
+
+
+@pytest.mark.parametrize("strategy", range(7))
+def test_residual_build_follows_fp64_closer_than_fp32(kh_fast, pkg, oracle, strategy):
+    """The FP32 build with residual planes (PackedResidual: FP32 slopes and
+    fluxes, the update in FP64 on hi + lo, the result split into the FP32
+    and 16-bit residual planes) through the single-problem kernels: after
+    15 steps its density is closer to the FP64 build's than the FP32
+    build's is, and its ring cells hold FP32 values exactly (the ghost
+    kernel zeroes their residuals).  Measured: 2.5e-9 to 3.1e-8 against
+    3.2e-8 to 9.0e-8 (relative L1) over the seven presets."""
+    nx, ny = 41, 30
+    U = pkg.scenarios.seeded_four_quadrant(nx, ny, 60 + strategy)
+    if strategy in (5, 6):
+        U = oracle.ghost(U, strategy)
+    kw = dict(width=1.0, height=0.7, t_end=0.02, cfl=0.45, alpha=ALPHA, gamma=GAMMA, strategy=strategy)
+    R = build_solve(kh_fast, 0, U, kw, 3, 15)
+    F32 = build_solve(kh_fast, 1, U, kw, 3, 15)
+    V = build_solve(kh_fast, 2, U, kw, 3, 15)
+    assert V[1] == R[1] and abs(V[2] - R[2]) <= 1e-6 * R[2]
+    inner = (slice(2, ny - 2), slice(2, nx - 2), 0)
+
+    def rel(A):
+        return np.abs(A[0][inner] - R[0][inner]).sum() / np.abs(R[0][inner]).sum()
+
+    print("preset", strategy, "FP32 with residuals", rel(V), "FP32", rel(F32))
+    assert rel(V) <= 1e-7 and rel(V) <= 0.7 * rel(F32), (rel(V), rel(F32))
+    ring = np.ones((ny, nx), bool)
+    ring[2:-2, 2:-2] = False
+    assert np.array_equal(V[0][ring], V[0][ring].astype(np.float32).astype(np.float64))
 
 
 def test_health_record_names_the_first_bad_step(kh, pkg):

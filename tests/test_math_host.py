@@ -88,6 +88,7 @@ def mh(tmp_path_factory):
 
     call.deriv = deriv
     call.count = count
+    call.lib = lib
     return call
 
 
@@ -187,7 +188,8 @@ def test_operations_per_cell_and_sweep(mh):
     """A cell's share of one sweep: one interface flux, four limited slopes,
     one update.  The shared-reciprocal slopes need no division and the
     update one (the reference's five); the compensated update adds
-    error-free sums and products but no division."""
+    error-free sums and products but no division, and applies 1/(gamma-1)
+    and gamma-1 with their low parts."""
     rng = np.random.default_rng(2)
     n = 500
     M = np.concatenate([cells(rng, n), cells(rng, n), cells(rng, n)], 1)
@@ -198,7 +200,7 @@ def test_operations_per_cell_and_sweep(mh):
         assert s0["div"] == s1["div"] == 0 and s1["mul"] <= s0["mul"]
         u0, u1, u2 = (mh.count(p, 3, pad(X[i])) for p in (REF, HOISTED, COMPENSATED))
         assert (u0["div"], u1["div"], u2["div"]) == (5, 1, 1)
-        assert u2["fma"] == 11  # the residuals of the two-products
+        assert u2["fma"] == 13  # the residuals of the two-products, the gamma constants' low parts
 
 
 def test_hoisted_flux_equals_reference_order(mh):
@@ -278,6 +280,48 @@ def test_updates_agree_and_compensation_helps_in_fp32(mh):
     # and smaller on average than the plain FP32 update for p, u and v
     # (measured 0.59, 0.64, 0.63 of it)
     assert np.all(comp.mean(0)[1:] <= 0.8 * plain.mean(0)[1:]), (comp.mean(0), plain.mean(0))
+
+
+def test_fp32_update_round_trip_keeps_pressure_unbiased(mh):
+    """With equal fluxes the update converts p to E and back.  The FP32
+    compensated update applies 1/(gamma-1) and gamma-1 with their low parts,
+    so the pressure returns without a drift; with the rounded constants
+    alone (2.5f and 1.4f - 1) every round trip scaled it by 1 - 6e-8, which
+    the tens of thousands of sweeps of a run accumulate."""
+    X = update_inputs(7)
+    X[:, 8:12] = X[:, 4:8]  # F_R = F_L
+    k32 = (float(np.float32(H)), float(np.float32(DT)), GAMMA, ALPHA)
+    ok = (X[:, 0] > 0) & (X[:, 1] > 0)
+    for policy in (COMPENSATED, PACKED):
+        P = mh("mh_update", policy, 32, X, k32)
+        rel = (P[ok, 1] - X[ok, 1]) / X[ok, 1]
+        print("policy", policy, "p round trip: mean signed", rel.mean(), "max", np.abs(rel).max())
+        assert abs(rel.mean()) <= 5e-9, rel.mean()
+        assert np.abs(rel).max() <= 3e-7
+
+
+def test_residual_storage_split(mh):
+    """The FP32 build with residual planes keeps x as hi = fl32(x) plus lo =
+    bf16(x - hi): hi + lo is within 2^-33 |x| of x, and splitting hi + lo
+    again gives the same bits, also where lo rounded to half a unit of hi's
+    last place (hi + lo then a tie between two FP32 values)."""
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(200_000) * np.exp(rng.uniform(-20, 20, 200_000))
+    hi = rng.standard_normal(20_000).astype(np.float32)
+    ulp = np.spacing(np.abs(hi)).astype(np.float64)
+    half = np.where(rng.random(20_000) < 0.5, 0.5, -0.5) * ulp
+    ties = hi.astype(np.float64) + half
+    # remainders just short of half a unit, which bf16 rounds up to it
+    near = hi.astype(np.float64) + half * (1.0 - 2.0 ** -12)
+    X = np.concatenate([x, ties, near])
+    lib = mh.lib
+    lib.mh_split.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+    out = np.empty((len(X), 3))
+    assert lib.mh_split(len(X), X.ctypes.data, out.ctypes.data) == 0
+    val = out[:, 0] + out[:, 1]
+    assert np.all(np.abs(val - X) <= 2.0 ** -33 * np.abs(X)), np.abs(val - X).max()
+    assert np.array_equal(val[len(x):len(x) + len(ties)], ties)  # a tie is held exactly
+    assert np.all(out[:, 2] == 1.0)
 
 
 def test_packed_fp32_physics_matches_the_scalar_form(mh):
