@@ -93,7 +93,8 @@ public:
     void setAlpha(double alpha) { alpha_ = alpha; }
     void setGamma(double gamma) { gamma_ = gamma; }
     void setGhostCellStrategy(ghostCellStrategy strategy) { strategy_ = strategy; }
-    // FVM2D_FP64 (default), FVM2D_FP64_STRICT, FVM2D_FP64_REFORDER or FVM2D_FP32; no reference counterpart.
+    // FVM2D_FP64 (default), FVM2D_FP64_STRICT, FVM2D_FP64_REFORDER, FVM2D_FP32 or FVM2D_FP32_RESIDUAL;
+    // no reference counterpart.
     void setPrecision(int precision) { precision_ = precision; }
     void setRecordModel(bool on_off, int gapPerFrame = 10, const std::string &recordDir = ".")
     {
