@@ -18,7 +18,13 @@ struct AdjointLaunch {
     const void *flux[4];   // interface fluxes of the sweeps X(U), Y(U), Y(A1), X(B1)
     const void *lb_out;    // adjoint of the step's output state
     void *lb_in;           // result: adjoint of the input state (may not alias lb_out)
-    void *work[3];         // work states
+    void *work[4];         // work states (the fourth used with a fork stream)
+    // optional: a second stream and two events of the caller's; branch B's
+    // first sweep transpose then runs on `fork` beside branch A's two, so
+    // the transposes fill each other's tail waves (also inside a graph
+    // capture, as parallel branches)
+    cudaStream_t fork = nullptr;
+    cudaEvent_t fork_ev[2] = {nullptr, nullptr};
 };
 
 #define FVM2D_DECLARE_ADJOINT(ns)                                                 \

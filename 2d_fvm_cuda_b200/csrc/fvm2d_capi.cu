@@ -189,6 +189,9 @@ struct fvm2d_solver {
     // buffer b filled, vjp_ev[2 + b] free again, vjp_ev[4] the start
     cudaStream_t aux = nullptr;
     cudaEvent_t vjp_ev[5] = {};
+    // the adjoint step's fork stream and events (AdjointLaunch::fork)
+    cudaStream_t fork = nullptr;
+    cudaEvent_t fork_ev[2] = {};
     std::vector<double> ck_t;     // time at each checkpoint
     double last_ms = 0.0;         // wall time of the last loop (the reference's timer)
     double last_device_ms = 0.0;  // CUDA-event time of the last loop on the stream
@@ -436,6 +439,12 @@ int fvm2d_destroy(fvm2d_solver *s)
     if (s->ev_end) cudaEventDestroy(s->ev_end);
     for (auto &e : s->vjp_ev)
         if (e) cudaEventDestroy(e);
+    for (auto &e : s->fork_ev)
+        if (e) cudaEventDestroy(e);
+    if (s->fork) {
+        cudaStreamSynchronize(s->fork);
+        cudaStreamDestroy(s->fork);
+    }
     if (s->aux) {
         cudaStreamSynchronize(s->aux);
         cudaStreamDestroy(s->aux);
@@ -1238,7 +1247,9 @@ static int segment_steps(int nsteps, int len, int count, int k)
     return k == 0 ? nsteps - (count - 1) * len : len;
 }
 
-constexpr int kAdjStates = 6;  // adjoint workspace: two adjoints, three work states, the saved final state
+// adjoint workspace: two adjoints, three work states, the saved final state,
+// the fourth work state of the fork stream's branch
+constexpr int kAdjStates = 7;
 
 // The adjoint step's launch parameters for this handle; the tape and
 // adjoint pointers are filled per step.
@@ -1259,7 +1270,20 @@ static fvm2d::AdjointLaunch adjoint_launch_of(const fvm2d_solver *s, size_t sb)
     L.gamma = s->gamma;
     L.dt = s->fixed_dt;
     for (int k = 0; k < 3; ++k) L.work[k] = s->adj + (2 + k) * sb;
+    L.work[3] = s->adj + 6 * sb;
+    L.fork = s->fork;
+    L.fork_ev[0] = s->fork_ev[0];
+    L.fork_ev[1] = s->fork_ev[1];
     return L;
+}
+
+// The adjoint step's fork stream and its events (created once per handle).
+static int ensure_fork(fvm2d_solver *s)
+{
+    if (s->fork) return FVM2D_OK;
+    CK(cudaStreamCreateWithFlags(&s->fork, cudaStreamNonBlocking));
+    for (auto &e : s->fork_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return FVM2D_OK;
 }
 
 // Enqueues on `st` the reverse of m steps taped in buffer `buf`, starting
@@ -1310,6 +1334,7 @@ static int vjp_workspace(fvm2d_solver *s, int *bufs)
     if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
     if (grew_tape || grew_adj) s->drop_vjp_graphs();
     if (grew_tape) s->last_taped = false;
+    if (int rc = ensure_fork(s)) return rc;
     if (*bufs == 2 && !s->aux) {
         // default priority: the recompute fills the SM room the reverse's
         // blocks leave (measured: at the device's higher priority the VJP
@@ -1418,6 +1443,7 @@ int fvm2d_vjp(fvm2d_solver *s, const double *cotangent_in, double *cotangent_out
         bool grew_adj;
         if (int rc = ensure(s->adj, s->adj_bytes, kAdjStates * sb, grew_adj)) return rc;
         if (grew_adj) s->drop_vjp_graphs();
+        if (int rc = ensure_fork(s)) return rc;
     } else if (int rc = vjp_workspace(s, &bufs)) {
         return rc;
     }
