@@ -1,7 +1,7 @@
 // fvm2d_split.cuh -- the storage of the FP32 build with residual planes: a
-// value x is kept as hi = x rounded to FP32 plus lo = (x - hi) rounded to
+// value x is kept as hi = x rounded to FP32 plus lo = (x - hi) cut to
 // bfloat16 (FP32's exponent range, 8 significant bits), so the stored value
-// carries about 32 significant bits in 6 bytes.  A state buffer holds the 4
+// carries about 31 significant bits in 6 bytes.  A state buffer holds the 4
 // FP32 planes (`plane` elements apart) followed by the residual block: for
 // each element offset o of a plane, the 4 fields' residuals as one 8-byte
 // word (16-bit residual of field f at index 4 o + f), so a sweep moves a
@@ -9,22 +9,12 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <string.h>
 
 namespace fvm2d {
 
-// bfloat16 bits of f, rounded to nearest with ties to even: the upper 16 bits
-// of f after adding half of the dropped part's unit (plus one when the kept
-// part is odd).  The residuals this stores are finite and small, so NaN and
-// overflow need no care here.
-__host__ __device__ inline unsigned short bf16_bits(float f)
-{
-    unsigned int u;
-    memcpy(&u, &f, 4);
-    u += 0x7fffu + ((u >> 16) & 1u);
-    return (unsigned short)(u >> 16);
-}
-
+// bfloat16 value of 16 bits: the upper half of an FP32 value.
 __host__ __device__ inline float bf16_value(unsigned short b)
 {
     const unsigned int u = (unsigned int)b << 16;
@@ -33,22 +23,25 @@ __host__ __device__ inline float bf16_value(unsigned short b)
     return f;
 }
 
-// hi + lo of x (hi rounded to nearest; lo the rounded remainder).  Where
-// the remainder rounds to half a unit of hi's last place, hi + lo lies
-// halfway between two FP32 values and rounding it to FP32 picks the even
-// one: that one is stored as hi (with the remainder taken from it), so that
-// splitting hi + lo again gives the same hi and lo -- a state read back and
-// set again continues bit for bit.  The stored value hi + lo is the same
-// either way.
+// hi + lo of x: hi = x rounded to nearest FP32; lo = x - hi (exact in FP64)
+// rounded toward zero to FP32 and truncated to bfloat16 (its upper 16 bits).
+// |lo| then stays below half a unit of hi's last place (or equals it where
+// x itself lies halfway, hi then even), so hi + lo rounds back to hi and
+// splitting it again gives the same hi and lo: a state read back and set
+// again continues bit for bit.  |x - (hi + lo)| < 2^-31 |x|.
 __host__ __device__ inline void split_value(double x, float &hi, unsigned short &lo)
 {
     hi = float(x);
-    lo = bf16_bits(float(x - double(hi)));
-    const float even = float(double(hi) + double(bf16_value(lo)));
-    if (even != hi) {
-        hi = even;
-        lo = bf16_bits(float(x - double(hi)));
-    }
+    const double r = x - double(hi);
+#if defined(__CUDA_ARCH__)
+    const float rf = __double2float_rz(r);
+#else
+    float rf = float(r);
+    if (fabs(double(rf)) > fabs(r)) rf = nextafterf(rf, 0.0f);
+#endif
+    unsigned int u;
+    memcpy(&u, &rf, 4);
+    lo = (unsigned short)(u >> 16);
 }
 
 __host__ __device__ inline double join_value(float hi, unsigned short lo) { return double(hi) + double(bf16_value(lo)); }

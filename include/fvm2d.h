@@ -62,8 +62,8 @@ enum fvm2d_precision {
                                 update; wave-speed max, dt and time stay FP64.  Host-side states
                                 remain doubles (converted on upload and download). */
     FVM2D_FP32_RESIDUAL = 4  /* FP32 slopes and fluxes; each stored value is an FP32 plane value
-                                plus a 16-bit (bfloat16) residual plane value, about 32
-                                significant bits in 6 bytes, and the conservative update runs
+                                plus a 16-bit (bfloat16) residual, about 31 significant bits
+                                in 6 bytes, and the conservative update runs
                                 in FP64 on hi + lo.  Solver handles only (no batches, no
                                 differentiation). */
 };

@@ -19,17 +19,17 @@ pytestmark = pytest.mark.gpu
 RHO_L1 = 1e-5  # density relative L1 against the FP64 path
 
 
-def bf16_round(x32):
-    """float32 values rounded to bfloat16 (to nearest, ties to even), as float32."""
-    u = np.ascontiguousarray(x32, dtype=np.float32).view(np.uint32).astype(np.uint64)
-    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
-    return (u.astype(np.uint32) << 16).view(np.float32)
-
-
 def stored(U):
-    """The value the residual storage keeps for each double of U."""
+    """The value the residual storage keeps for each double of U: hi = U
+    rounded to FP32, plus U - hi rounded toward zero to FP32 and cut to its
+    upper 16 bits (bfloat16)."""
     hi = U.astype(np.float32).astype(np.float64)
-    return hi + bf16_round((U - hi).astype(np.float32)).astype(np.float64)
+    r = U - hi
+    rf = r.astype(np.float32)
+    over = np.abs(rf.astype(np.float64)) > np.abs(r)
+    rf[over] = np.nextafter(rf[over], np.float32(0))
+    lo = (rf.view(np.uint32) & np.uint32(0xFFFF0000)).view(np.float32)
+    return hi + lo.astype(np.float64)
 
 
 def run(pkg, U0, precision, steps=None, **kw):
