@@ -124,14 +124,13 @@ struct PackedResidual : PackedCompensated {
         const double igm1 = double(K.igm1) + double(K.igm1_lo), gm1 = double(K.gm1) + double(K.gm1_lo);
         double m0 = rho, m1 = rho * un, m3 = rho * ut;
         double m2 = fma(p, igm1, 0.5 * (m1 * un + m3 * ut));
-        // W - lambda (F_R - F_L), the flux differences taken in FP32 (exact
-        // where the two fluxes are within a factor 2 of each other, as in
-        // smooth flow; measured: the same 2000^2 vortex result as FP64
-        // differences, 1% faster)
-        m0 = fma(double(FL.rho - FR.rho), lam, m0);
-        m1 = fma(double(FL.p - FR.p), lam, m1);
-        m2 = fma(double(FL.un - FR.un), lam, m2);
-        m3 = fma(double(FL.ut - FR.ut), lam, m3);
+        // W - lambda (F_R - F_L), the flux differences exact in FP64 (FP32
+        // differences measured 1% faster, but across the jet's strong
+        // gradients they doubled this build's distance from FP64)
+        m0 = fma(double(FL.rho) - double(FR.rho), lam, m0);
+        m1 = fma(double(FL.p) - double(FR.p), lam, m1);
+        m2 = fma(double(FL.un) - double(FR.un), lam, m2);
+        m3 = fma(double(FL.ut) - double(FR.ut), lam, m3);
         const double ir = rrcp(m0);
         Cell<double> o;
         o.rho = m0;
