@@ -3,7 +3,7 @@ its own libfvm2d solver holding a slab plus halo rows, exchanging rows
 through host memory between steps (gloo).  The gathered result must equal a
 single solver's run of the whole array bit for bit, including the presets
 whose ghost rules use global row numbers (jet rows, the double-Mach shock
-position).  The NCCL path, whose steps are enqueued on the device with no
+position), in the FP64, FP32 and residual builds (the rows carry hi + lo).  The NCCL path, whose steps are enqueued on the device with no
 host round trip (asynchronous row transfers, device-side max reduction and
 step plan), runs as one rank on the one GPU and must equal the single
 solver bit for bit too."""
@@ -37,7 +37,7 @@ def single(pkg, case):
 
 
 CASES = [dict(world=w, nx=48, ny=53, seed=10 + s, strategy=s, width=1.0, height=1.1, t_end=0.03, precision=p)
-         for w, s, p in [(2, 0, 1), (3, 2, 1), (2, 3, 1), (3, 4, 1), (3, 5, 1), (2, 6, 0)]]
+         for w, s, p in [(2, 0, 1), (3, 2, 1), (2, 3, 1), (3, 4, 1), (3, 5, 1), (2, 6, 0), (2, 1, 4)]]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"world{c['world']}-strategy{c['strategy']}-prec{c['precision']}")
@@ -51,7 +51,7 @@ def test_gpu_slabs_equal_single_solver(pkg, case, tmp_path):
     assert np.array_equal(G, V, equal_nan=True)
 
 
-@pytest.mark.parametrize("precision", [0, 3])
+@pytest.mark.parametrize("precision", [0, 3, 4])
 def test_rows_round_trip_through_host_and_device_memory(pkg, precision):
     import torch
 
@@ -75,7 +75,7 @@ def test_rows_round_trip_through_host_and_device_memory(pkg, precision):
 
 
 NCCL_CASES = [dict(world=1, nx=96, ny=80, seed=3, strategy=s, width=1.0, height=0.9, t_end=0.05, precision=p, first=7)
-              for s, p in [(0, 0), (5, 0), (4, 3), (2, 1)]]
+              for s, p in [(0, 0), (5, 0), (4, 3), (2, 1), (6, 4)]]
 
 
 @pytest.mark.parametrize("case", NCCL_CASES, ids=lambda c: f"strategy{c['strategy']}-prec{c['precision']}")
