@@ -479,9 +479,10 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
             c0 = ld(c);
             cp1 = ld(c + 1);
         }
-        Cell<Real> A, Alo;
+        Cell<Real> A, Alo, Ulo;
         if (FINAL) A = load_cell(a.comb, min(max(u, 0), nx - 1), y, 2, 3);  // branch A, loaded early
         if (FINAL && kResidual) Alo = load_lo(a.comb, min(max(u, 0), nx - 1), y, 2, 3);
+        if (kResidual) Ulo = load_lo(a.src, min(max(u, 0), nx - 1), y, 2, 3);  // the updated cell's, early
         const Cell<Real> s0 = Phys::slope(cm1, c0, cp1, K);                // slope of cell c
         Cell<Real> sm1 = shfl_up(s0);                                     // slope of cell c-1
         if (lane == 0) sm1 = cs;
@@ -492,7 +493,7 @@ __device__ __forceinline__ void x_item(const SweepArgs<Real> &a, const SweepCons
         if (lane == 0) FL = cF;
         if ((j > 0 || lane >= 2) && u <= last) {
             if constexpr (kResidual)
-                emit_split(u, Phys::update_split(cm1, load_lo(a.src, u, y, 2, 3), FL, F, K), join_cell(A, Alo));
+                emit_split(u, Phys::update_split(cm1, Ulo, FL, F, K), join_cell(A, Alo));
             else
                 emit(u, Phys::update(cm1, FL, F, K), A);
         }
@@ -570,7 +571,8 @@ constexpr int kYRingRows = 8;
 
 template <typename Real, class Phys, int RING = 0>
 __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepConsts<Real> &K, int seg, int nseg,
-                                       int cw, int lane, int T, Real *ring = nullptr, int rs = 0)
+                                       int cw, int lane, int T, Real *ring = nullptr, int rs = 0,
+                                       unsigned long long *ring_lo = nullptr)
 {
     const int nx = a.nx, ny = a.ny;
     const bool tape = a.flux.base != nullptr;  // as in x_item
@@ -612,6 +614,13 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
             async_copy(r + rs, &a.src.at(1, xc, y));
             async_copy(r + 2 * rs, &a.src.at(3, xc, y));
             async_copy(r + 3 * rs, &a.src.at(2, xc, y));
+            // residual builds: the row's residual word rides in the ring too
+            if constexpr (kResidual) async_copy(ring_lo + (l & (kYRingRows - 1)) * rs, &lo_cell(a.src, xc, y));
+        };
+        auto get_lo = [&](int l) {  // the residuals of row l, in (rho, p, un, ut) order
+            const unsigned long long w = ring_lo[(l & (kYRingRows - 1)) * rs];
+            auto part = [&](int f) { return Real(bf16_value((unsigned short)(w >> (16 * f)))); };
+            return Cell<Real>{part(0), part(1), part(3), part(2)};
         };
         auto get = [&](int l) {
             const Real *r = ring + (l & (kYRingRows - 1)) * 4 * rs;
@@ -641,7 +650,7 @@ __device__ __forceinline__ void y_item(const SweepArgs<Real> &a, const SweepCons
             if (tape && col) store_cell(a.flux, x, ny - 1 - l, 2, 3, F);
             if (l > l0 && col) {
                 if constexpr (kResidual)
-                    store_split(a.dst, x, ny - l, 3, 2, Phys::update_split(cm1, load_lo(a.src, x, ny - l, 3, 2), Fp, F, K));
+                    store_split(a.dst, x, ny - l, 3, 2, Phys::update_split(cm1, get_lo(l - 1), Fp, F, K));
                 else
                     store_cell(a.dst, x, ny - l, 3, 2, Phys::update(get(l - 1), Fp, F, K));
             }
@@ -679,7 +688,13 @@ __global__ void __launch_bounds__(NT, MINB) sweep_y_kernel(SweepArgs<Real> a, in
     const long long nwork = (long long)ncw * nseg;
     const long long wstride = (long long)gridDim.x * (NT / 32);
     constexpr int RING = (sizeof(Real) == 4 || sizeof(Real) == 8) ? FVM2D_Y_RING : 0;
-    if constexpr (RING > 0) {
+    if constexpr (RING > 0 && split_storage<Phys>::value) {
+        __shared__ Real ring[kYRingRows * 4 * NT];
+        __shared__ unsigned long long ring_lo[kYRingRows * NT];
+        for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
+            y_item<Real, Phys, RING>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T, ring + threadIdx.x, NT,
+                                     ring_lo + threadIdx.x);
+    } else if constexpr (RING > 0) {
         __shared__ Real ring[kYRingRows * 4 * NT];
         for (long long w = (long long)blockIdx.x * (NT / 32) + threadIdx.x / 32; w < nwork; w += wstride)
             y_item<Real, Phys, RING>(a, K, int(w / ncw), nseg, int(w % ncw), lane, T, ring + threadIdx.x, NT);
