@@ -176,11 +176,11 @@ struct fvm2d_solver {
     size_t ck_bytes = 0, tape_bytes = 0, adj_bytes = 0;
     int ck_count = 0, ck_len = 0, fwd_steps = -1, fwd_precision = -1;
     bool full_tape = false;       // the last fvm2d_forward kept every step's tape
-    // fvm2d_vjp's graphs for a full segment: its taped recompute into tape
-    // buffer b ([b]), and its reverse from tape buffer b starting from
-    // adjoint buffer a ([2 + 2b + a]); built for vjp_len steps and vjp_bufs
-    // tape buffers
-    cudaGraphExec_t vjp_graph[6] = {};
+    // the graphs of a full checkpoint segment: its taped recompute into tape
+    // buffer b ([b]), its reverse from tape buffer b starting from adjoint
+    // buffer a ([2 + 2b + a]), and its untaped forward steps ([6], for
+    // fvm2d_forward); built for vjp_len steps and vjp_bufs tape buffers
+    cudaGraphExec_t vjp_graph[7] = {};
     int vjp_len = 0, vjp_bufs = 0;
     bool last_taped = false;      // the checkpointed forward taped its last segment (fvm2d_vjp skips its recompute)
     bool vjp_overlap = true;      // fvm2d_set_vjp_overlap: two tape buffers where they fit
@@ -1349,6 +1349,11 @@ static int vjp_workspace(fvm2d_solver *s, int *bufs)
         CK(is_fp32(s->precision) ? fvm2d::adj32::adjoint_prepare() : fvm2d::adj::adjoint_prepare());
         const LaunchConfig c = s->config();
         const int len = s->ck_len;
+        if (int rc = s->capture(&s->vjp_graph[6], [&] {
+                for (int j = 0; j < len; ++j) CK(kVariants[s->precision].step(c, s->stream, nullptr));
+                return FVM2D_OK;
+            }))
+            return rc;
         for (int b = 0; b < *bufs; ++b) {
             if (int rc = s->capture(&s->vjp_graph[b], [&] { return taped_steps(s, c, len, b, s->stream); }))
                 return rc;
@@ -1409,6 +1414,11 @@ int fvm2d_forward(fvm2d_solver *s, int nsteps, int checkpoints)
             } else if (int rc = taped_steps(s, c, m, b, s->stream)) {
                 return rc;
             }
+            for (int q = 0; q < m; ++q) t = t + s->fixed_dt;
+            continue;
+        }
+        if (count > 1 && m == s->vjp_len) {  // a full segment: one graph of its steps
+            CK(cudaGraphLaunch(s->vjp_graph[6], s->stream));
             for (int q = 0; q < m; ++q) t = t + s->fixed_dt;
             continue;
         }
