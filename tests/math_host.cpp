@@ -259,6 +259,28 @@ int mh_slope(int policy, int bits, long n, const double *in, const double *k4, d
     return 1;
 }
 
+// The limiter of one component, n triples (m, c, p) in `in` (n x 3), with
+// hrh, rha in k2: out n x 2 = (the form the sweeps compile for the type --
+// the double or float overload --, the generic template form).  bits 64 or
+// 32.
+int mh_limiter_forms(int bits, long n, const double *in, const double *k2, double *out)
+{
+    for (long i = 0; i < n; ++i) {
+        const double *q = in + 3 * i;
+        if (bits == 64) {
+            out[2 * i] = limited_slope_hoisted(q[0], q[1], q[2], k2[0], k2[1]);
+            out[2 * i + 1] = limited_slope_hoisted<double>(q[0], q[1], q[2], k2[0], k2[1]);
+        } else if (bits == 32) {
+            const float m = float(q[0]), c = float(q[1]), p = float(q[2]), a = float(k2[0]), b = float(k2[1]);
+            out[2 * i] = limited_slope_hoisted(m, c, p, a, b);
+            out[2 * i + 1] = limited_slope_hoisted<float>(m, c, p, a, b);
+        } else {
+            return 1;
+        }
+    }
+    return 0;
+}
+
 // ---- derivatives (FP64, shared-reciprocal forms) ----------------------------
 // Tangents (dual numbers through Hoisted) and adjoints (the hand-written
 // reverse the VJP kernels run) of the same maps, one interface or cell per

@@ -364,6 +364,44 @@ def test_hoisted_limiter_picks_the_reference_zero_pattern(mh):
     assert (np.abs(S1 - S0)[nz] / np.abs(S0[nz])).max() <= 4e-7  # measured 1.1e-7
 
 
+def limiter_triples(rng, n):
+    """(m, c, p) triples that reach every corner of the limiter: equal
+    neighbours, differences at the rounding of the values, subnormal and
+    underflowing products, overflowing ones, signed zeros, infinities and
+    NaN, besides ordinary data."""
+    scale = 10.0 ** rng.uniform(-320, 300, (n, 1))
+    X = rng.standard_normal((n, 3)) * scale
+    c = rng.uniform(0.1, 3.0, n)
+    near = np.stack([c - rng.integers(-3, 4, n) * np.spacing(c), c, c + rng.integers(-3, 4, n) * np.spacing(c)], 1)
+    special = np.array([0.0, -0.0, 5e-324, -5e-324, 1e-160, 1e160, np.inf, -np.inf, np.nan, 1.0, -1.0, 2.5])
+    S = special[rng.integers(0, len(special), (n, 3))]
+    mix = np.where(rng.random((n, 3)) < 0.5, S, X)
+    return np.concatenate([X, near, S, mix])
+
+
+def test_limiter_overloads_equal_the_generic_form(mh):
+    """The sweeps' double and float limiters test d1 d2 > 0 alone (d1 d2 > 0
+    implies dc d2 > 0) and take the sign of dc by copysign: the same bits as
+    the generic form with both tests, on ordinary and degenerate inputs."""
+    lib = mh.lib
+    lib.mh_limiter_forms.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.mh_limiter_forms.restype = ctypes.c_int
+    rng = np.random.default_rng(21)
+    X = np.ascontiguousarray(limiter_triples(rng, 200_000))
+    for bits, k2 in ((64, (200.0, 380.0)), (64, (0.5, 1.9)), (64, (1e300, 1e-300)), (32, (200.0, 380.0))):
+        k = np.asarray(k2, dtype=np.float64)
+        out = np.empty((len(X), 2))
+        with np.errstate(all="ignore"):
+            assert lib.mh_limiter_forms(bits, len(X), X.ctypes.data, k.ctypes.data, out.ctypes.data) == 0
+        fast, generic = out[:, 0], out[:, 1]
+        if bits == 32:  # the float overload's min instructions differ from selects on NaN arguments only
+            with np.errstate(all="ignore"):
+                keep = ~np.isnan(X.astype(np.float32)).any(1)
+            fast, generic = fast[keep], generic[keep]
+        assert np.array_equal(fast.view(np.int64), generic.view(np.int64)), (bits, k2)
+        assert (generic != 0).mean() > 0.05
+
+
 def dot_mismatch(Jv, w, v, JTw):
     """Per row |<Jv, w> - <v, J^T w>| over the sum of the magnitudes of the
     terms of both dot products."""
