@@ -22,11 +22,11 @@ struct Cell5 {
 // ---- limiter -------------------------------------------------------------
 // s = Hoisted::slope's limiter (limited_slope_hoisted) on (m, c, p): which
 // difference was selected (0 none, 1 central, 2 backward, 3 forward), for the
-// adjoint.  Same tests and tie order.
+// adjoint.  Same tests and tie order (d1 d2 > 0 alone: it implies dc d2 > 0).
 __device__ __forceinline__ int slope_choice(A m, A c, A p, A rh, A alpha)
 {
     const A d1 = c - m, d2 = p - c, dc = p - m;
-    if (!(dc * d2 > A(0) && d1 * d2 > A(0))) return 0;
+    if (!(d1 * d2 > A(0))) return 0;
     const A a1 = fabs(d1), a2 = fabs(d2);
     const A inner = (rh * alpha) * ((a2 < a1) ? a2 : a1);
     if (!(inner < fabs(dc) * (rh * A(0.5)))) return 1;

@@ -353,12 +353,13 @@ def product_arm(args, rank, world, local_rank):
                 except Exception as e:  # noqa: BLE001
                     fp32_configs[key] = {"error": f"{type(e).__name__}: {e}"}
         # the batched form on its workload (256 uneven four-quadrant problems),
-        # FP64, against the same problems solved one at a time
+        # FP64 and FP32, against the same problems solved one at a time
         batch = None
         if world == 1 and not args.no_configs:
             try:
-                batch = _batch_case(pkg, pkg.scenarios.uneven_batch(256, 3), ((pkg.FP64, "fp64"),),
-                                    "256 problems, sides 128..1024")[0]
+                b64, b32 = _batch_case(pkg, pkg.scenarios.uneven_batch(256, 3),
+                                       ((pkg.FP64, "fp64"), (pkg.FP32, "fp32")), "256 problems, sides 128..1024")
+                batch = dict(b64, fp32=b32)
             except Exception as e:  # noqa: BLE001
                 batch = {"error": f"{type(e).__name__}: {e}"}
         out = {
@@ -630,6 +631,10 @@ def adjoint_summary(pkg):
     best = timed(pkg.FULL_TAPE)
     ck = timed(15)  # ceil(sqrt(200)) checkpoints, each segment recomputed by the VJP
     ck1 = timed(15, overlap=False)  # one tape buffer: recompute and reverse in turn
+    try:  # the timings above stand even if a check fails to run
+        checks = adjoint_checks(pkg, h, U, n, steps, hh)
+    except Exception as e:  # noqa: BLE001
+        checks = {"error": f"{type(e).__name__}: {e}"}
     h.close()
     f = min(fwd[1:])
     return {"workload": "512^2 periodic vortex + 16 density modes, 200 fixed-dt steps, FP64",
@@ -643,7 +648,54 @@ def adjoint_summary(pkg):
                              "one_buffer": {"forward_ms": ck1[0], "vjp_ms": ck1[1],
                                             "forward_plus_adjoint_over_forward": sum(ck1) / f}},
             "forward_plus_adjoint_over_forward": sum(best) / f,
-            "checkpointed_ratio": sum(ck) / f}
+            "checkpointed_ratio": sum(ck) / f,
+            "checks": checks}
+
+
+def adjoint_checks(pkg, h, U, n, steps, hh):
+    """The gradient checks of the differentiation workload at its full size
+    (512^2, 200 steps, the handle's fixed dt): the gradient of
+    J = sum (rho_T - rho_target)^2 (target from a second seeded perturbation)
+    by the VJP with 15 checkpoints against central differences along six
+    smooth density modes, and the same directional derivative by the
+    tangent-linear run (fvm2d_jvp): <dJ/drho_T, J d> = <J^T dJ/drho_T, d>,
+    the dot-product identity of the JVP and the VJP."""
+    import math
+    sc = pkg.scenarios
+
+    def final(U0):
+        h.set_state(U0)
+        h.advance(steps)
+        return h.get_state(4)
+
+    target = final(sc.isentropic_vortex(n, perturbation=sc.density_modes(16, 1e-3, 11)))[..., 0]
+    h.set_state(U)
+    h.forward(steps, 15)
+    cot = np.zeros_like(U)
+    cot[..., 0] = 2 * (h.get_state(4)[..., 0] - target)
+    grad = h.vjp(cot)[..., 0]
+
+    def J(U0):
+        return math.fsum(((final(U0)[..., 0] - target) ** 2).ravel())
+
+    xs = (np.arange(n) - 2 + 0.5) * hh
+    X, Y = np.meshgrid(xs, 10.0 - xs)
+    d = np.zeros_like(U)
+    d[..., 0] = sc.density_modes(6, 1.0, 20)(X, Y)
+    eps = 1e-8
+    fd = (J(U + eps * d) - J(U - eps * d)) / (2 * eps)
+    ad = float(np.sum(grad * d[..., 0]))
+    # the same derivative in forward mode, <dJ/drho_T, JVP(d)>, from the
+    # dual-number build (which rounds on its own)
+    h.set_state(U)
+    tl = float(np.sum(cot[..., 0] * h.jvp(steps, d)[..., 0]))
+    return {"objective": "J = sum (rho_T - rho_target)^2, 15 checkpoints",
+            "direction": "6 smooth density modes",
+            "fd": {"eps": eps, "value": fd, "rel_diff_vs_adjoint": abs(fd - ad) / abs(ad), "target": 1e-5},
+            "adjoint": ad,
+            "tangent_linear": {"value": tl, "rel_diff_vs_adjoint": abs(tl - ad) / abs(ad),
+                               "what": "<dJ/drho_T, JVP(d)> = <d, VJP(dJ/drho_T)>: the dot-product identity "
+                                       "of the JVP and the VJP on these smooth directions"}}
 
 
 def form_adjoint(args):
