@@ -649,7 +649,9 @@ def adjoint_summary(pkg):
                                             "forward_plus_adjoint_over_forward": sum(ck1) / f}},
             "forward_plus_adjoint_over_forward": sum(best) / f,
             "checkpointed_ratio": sum(ck) / f,
-            "checks": checks}
+            "checks": checks,
+            "preset_parity": "periodic is not a reference preset: its ghost rule is pinned to the oracle's "
+                             "restatement only"}
 
 
 def adjoint_checks(pkg, h, U, n, steps, hh):
