@@ -43,6 +43,7 @@ SIGNATURES = [
     ("fvm2d_solve", ctypes.c_int, [_vp]),
     ("fvm2d_advance", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("fvm2d_get_health", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
+    ("fvm2d_get_conserved_totals", ctypes.c_int, [_vp, _dp]),
     ("fvm2d_set_record_model", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
     ("fvm2d_write_frame_png", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("fvm2d_write_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
@@ -248,6 +249,13 @@ class Handle:
         k = ctypes.c_int(0)
         check(self.lib.fvm2d_get_health(self.h, ctypes.byref(k)))
         return k.value
+
+    def conserved_totals(self) -> np.ndarray:
+        """Mass, x momentum, y momentum and energy of the interior cells, in
+        FP64 whatever the precision (fvm2d_get_conserved_totals)."""
+        out = np.zeros(4)
+        check(self.lib.fvm2d_get_conserved_totals(self.h, out.ctypes.data_as(_dp)))
+        return out
 
     # -- frames and state files --
     def set_record_model(self, on: bool, gap_per_frame: int = 10, record_dir: str = ".") -> None:

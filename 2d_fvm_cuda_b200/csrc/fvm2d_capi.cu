@@ -23,6 +23,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include <algorithm>
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -36,6 +37,8 @@
 using fvm2d::LaunchConfig;
 using fvm2d::StepControl;
 using fvm2d::aos_to_soa;
+using fvm2d::conserved_partials;
+using fvm2d::conserved_sum;
 using fvm2d::convert_planes;
 using fvm2d::is_device_pointer;
 using fvm2d::rows_in;
@@ -952,6 +955,32 @@ int fvm2d_get_health(fvm2d_solver *s, int *first_bad_step)
     if (int rc = check(s)) return rc;
     if (!first_bad_step) return fail(FVM2D_ERR_INVALID, "null output pointer");
     *first_bad_step = s->ctl_h->first_bad;
+    return FVM2D_OK;
+}
+
+int fvm2d_get_conserved_totals(fvm2d_solver *s, double *totals)
+{
+    Range range_("fvm2d_get_conserved_totals");
+    if (int rc = check(s)) return rc;
+    if (!totals) return fail(FVM2D_ERR_INVALID, "null output pointer");
+    if (!s->have_state) return fail(FVM2D_ERR_STATE, "no state has been set");
+    constexpr int NT = 256;
+    const long long cells = (long long)(s->nx - 4) * (s->ny - 4);
+    const int blocks = (int)std::min<long long>(148 * 4, (cells + NT - 1) / NT);
+    // the per-block partials, then the totals, in the sweep buffers (idle
+    // between steps; everything runs in order on the handle's stream)
+    double *partial = s->scratch, *sum = s->scratch + 4 * (long long)blocks;
+    with_planes(s->precision, s->U, s->plane, [&](auto st) {
+        conserved_partials<decltype(st), NT>
+            <<<blocks, NT, 0, s->stream>>>(st, s->nx, s->ny, s->pitch, s->plane, s->gamma, partial);
+    });
+    CK(cudaGetLastError());
+    const LaunchConfig c = s->config();
+    conserved_sum<<<1, 32, 0, s->stream>>>(partial, blocks, c.hx * c.hy, sum);
+    CK(cudaGetLastError());
+    const cudaMemcpyKind kind = is_device_pointer(totals) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(totals, sum, 4 * sizeof(double), kind, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
     return FVM2D_OK;
 }
 

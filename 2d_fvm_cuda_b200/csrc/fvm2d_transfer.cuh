@@ -67,6 +67,56 @@ static __global__ void rows_in(S U, long long plane, int pitch, int j0, int nrow
     }
 }
 
+// Conserved totals of the interior cells (rows and columns 2 .. n-3, the
+// cells the sweeps update): per block, the sums of rho, rho u, rho v and
+// E = p / (gamma - 1) + rho (u^2 + v^2) / 2 in FP64 whatever the storage,
+// written to partial[4 * block + f]; conserved_sum then adds the blocks in
+// block order.  Cells are dealt to threads by a fixed grid-stride and the
+// block sums follow a fixed tree, so a state gives the same bits on every
+// call with the same grid.  NT is the block size (a power of two).
+template <class S, int NT>
+static __global__ void __launch_bounds__(NT) conserved_partials(S U, int nx, int ny, int pitch, long long plane,
+                                                                double gamma, double *__restrict__ partial)
+{
+    __shared__ double red[4][NT];
+    const int t = threadIdx.x;
+    const int iw = nx - 4;
+    const long long n = (long long)iw * (ny - 4);
+    const double igm1 = 1.0 / (gamma - 1.0);
+    double m = 0.0, mu = 0.0, mv = 0.0, e = 0.0;
+    for (long long k = blockIdx.x * (long long)NT + t; k < n; k += (long long)gridDim.x * NT) {
+        const long long o = (long long)(2 + k / iw) * pitch + (2 + k % iw);
+        const double rho = U.get(o), p = U.get(plane + o), u = U.get(2 * plane + o), v = U.get(3 * plane + o);
+        m += rho;
+        mu += rho * u;
+        mv += rho * v;
+        e += p * igm1 + 0.5 * rho * (u * u + v * v);
+    }
+    red[0][t] = m;
+    red[1][t] = mu;
+    red[2][t] = mv;
+    red[3][t] = e;
+    __syncthreads();
+    for (int s = NT / 2; s > 0; s >>= 1) {
+        if (t < s)
+            for (int f = 0; f < 4; ++f) red[f][t] += red[f][t + s];
+        __syncthreads();
+    }
+    if (t < 4) partial[4 * blockIdx.x + t] = red[t][0];
+}
+
+// totals[f] = area * sum over blocks b (in order) of partial[4 b + f]; one
+// thread per total.
+static __global__ void conserved_sum(const double *__restrict__ partial, int nblocks, double area,
+                                     double *__restrict__ totals)
+{
+    const int f = threadIdx.x;
+    if (f >= 4) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[4 * b + f];
+    totals[f] = s * area;
+}
+
 inline bool is_device_pointer(const void *p)
 {
     cudaPointerAttributes a;

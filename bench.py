@@ -827,12 +827,17 @@ def form_vortex(args, with_reference_order=False):
         h = pkg.Handle(n, n)
         h.configure(w, hgt, 10.0, 0.45, 1.9, 1.4, 5, prec)
         h.set_state(U0)
+        before = h.conserved_totals()
         h.solve()
         ms, _ = h.run_stats()
         t, steps, _ = h.time()
+        after = h.conserved_totals()
         states[name] = h.get_state(4)
         h.close()
-        res[name] = {"steps": steps, "t": t, "device_s": ms / 1e3, "cell_updates_per_s": n * n * steps / (ms / 1e3)}
+        res[name] = {"steps": steps, "t": t, "device_s": ms / 1e3, "cell_updates_per_s": n * n * steps / (ms / 1e3),
+                     # FP64 totals of the interior (fvm2d_get_conserved_totals) over the period
+                     "conserved_rel_change": {"fields": ["mass", "x momentum", "y momentum", "energy"],
+                                              "value": [float(x) for x in np.abs(after - before) / np.abs(before)]}}
     E = sc.isentropic_vortex(n, t=res["fp64"]["t"])
     inner = (slice(2, n - 2), slice(2, n - 2))
 

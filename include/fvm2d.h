@@ -156,6 +156,18 @@ int fvm2d_advance(fvm2d_solver *s, int nsteps, int *steps_done);
  * way, as the reference's does. */
 int fvm2d_get_health(fvm2d_solver *s, int *first_bad_step);
 
+/* Conserved totals of the current state (no reference counterpart: the
+ * reference has no diagnostics).  totals[0..3] (host or device memory)
+ * receive the mass, x momentum, y momentum and energy of the interior cells
+ * (rows and columns 2 .. n-3; for a row slab, its own rows), each the sum of
+ * rho, rho u, rho v and p / (gamma - 1) + rho (u^2 + v^2) / 2 times the cell
+ * area, computed in FP64 whatever the precision of the state, in a fixed
+ * order: the same state gives the same bits.  The split step conserves the
+ * mass exactly up to rounding; momentum and energy only up to the average of
+ * the two split orders being taken in primitive variables
+ * (src/basicFuns.cuh:264-274). */
+int fvm2d_get_conserved_totals(fvm2d_solver *s, double *totals);
+
 /* ---- frames and state files -----------------------------------------------
  * Frame recording replaces RGRP_2D_CUDA::setRecordModel / writeStagesTo_png
  * (src/wrappers.cuh:147-152, 253-260, 323-345): with recording on,

@@ -22,6 +22,7 @@
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_packed.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_batch.cuh"
 #include "../2d_fvm_cuda_b200/csrc/fvm2d_io.cuh"
+#include "../2d_fvm_cuda_b200/csrc/fvm2d_transfer.cuh"
 
 using namespace fvm2d::host;
 using fvm2d::ad::Dual;
@@ -500,6 +501,40 @@ int kh_frame(const double *cells, int nx, int ny, int blocks, const char *path)
         fvm2d::io::render_density<double>(rho.data(), pitch, nx, ny, parts.data(), blocks, rgb.data());
     });
     return fvm2d::io::write_png_rgb(path, nx, ny, rgb.data()) ? 0 : 2;
+}
+
+// The conserved totals as fvm2d_get_conserved_totals computes them
+// (conserved_partials over `blocks` blocks of 256 threads, then
+// conserved_sum) on a (ny, nx, 4) array of (rho, p, u, v) cells, stored
+// first as the solver stores them: storage 0 FP64 planes, 1 FP32 planes,
+// 2 FP32 planes with residuals, rows `pitch` elements apart.  totals: mass,
+// x momentum, y momentum, energy times `area`.
+int kh_totals(const double *cells, int nx, int ny, int pitch, int storage, int blocks, double gamma, double area,
+              double *totals)
+{
+    constexpr int kNT = 256;
+    if (nx < 6 || ny < 6 || pitch < nx || blocks < 1 || storage < 0 || storage > 2) return 1;
+    const long long plane = (long long)pitch * ny;
+    std::vector<double> d(storage == 0 ? 4 * plane : 0);
+    std::vector<float> f(storage == 0 ? 0 : 6 * plane);  // FP32 planes, then room for the residual block
+    std::vector<double> partial(4 * (size_t)blocks), sum(4);
+    auto run = [&](auto st) {
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x)
+                for (int q = 0; q < 4; ++q) st.put(q * plane + (long long)y * pitch + x, cells[4 * ((size_t)y * nx + x) + q]);
+        emu::launch(dim3(blocks), dim3(kNT), true, [&] {
+            fvm2d::conserved_partials<decltype(st), kNT>(st, nx, ny, pitch, plane, gamma, partial.data());
+        });
+        emu::launch(dim3(1), dim3(32), false, [&] { fvm2d::conserved_sum(partial.data(), blocks, area, sum.data()); });
+    };
+    if (storage == 0)
+        run(fvm2d::Planes<double>{d.data()});
+    else if (storage == 1)
+        run(fvm2d::Planes<float>{f.data()});
+    else
+        run(fvm2d::split_planes(f.data(), plane));
+    for (int q = 0; q < 4; ++q) totals[q] = sum[q];
+    return 0;
 }
 
 } // extern "C"

@@ -90,6 +90,7 @@ def _kernels_host(tmp_path_factory, defines=()):
     lib.kh_sweep32.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 + [ctypes.c_double] * 4
     lib.kh_step_jvp.argtypes = STEP_ARGS + [ctypes.c_void_p] * 2
     lib.kh_step_vjp.argtypes = STEP_ARGS + [ctypes.c_void_p]
+    lib.kh_totals.argtypes = ([ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_double] * 2 + [ctypes.c_void_p])
     return lib
 
 
@@ -500,3 +501,47 @@ def test_fp32_adjoint_kernels_agree_with_fp64(kh, k32, oracle, pkg, strategy):
     assert k32.k32_step_vjp(U.ctypes.data, w.ctypes.data, *args, g32.ctypes.data) == 0
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     assert rel <= 1e-4, rel
+
+
+@pytest.mark.parametrize("nx,ny,pitch,blocks", [(37, 29, 64, 1), (64, 48, 64, 3), (70, 33, 96, 2)])
+def test_conserved_totals_kernels(kh, nx, ny, pitch, blocks):
+    """fvm2d_get_conserved_totals' kernels (csrc/fvm2d_transfer.cuh) on the
+    host: the interior totals of mass, momenta and energy in FP64 for each
+    storage (FP64 planes, FP32 planes, FP32 planes with residuals), against
+    exactly summed totals of the values each storage holds; the ghost ring
+    (set to huge values here) is left out; the same state gives the same bits."""
+    import math
+    rng = np.random.default_rng(nx * ny)
+    U = np.empty((ny, nx, 4))
+    U[..., 0] = rng.uniform(0.1, 2.0, (ny, nx))
+    U[..., 1] = rng.uniform(0.02, 2.0, (ny, nx))
+    U[..., 2:] = rng.uniform(-1.5, 1.5, (ny, nx, 2))
+    ring = np.ones((ny, nx), bool)
+    ring[2:-2, 2:-2] = False
+    U[ring] = 1e30
+    gamma, area = 1.4, 0.37
+
+    def held(storage):  # the values the storage keeps, as FP64
+        if storage == 0:
+            return U
+        if storage == 1:
+            return U.astype(np.float32).astype(np.float64)
+        hi = U.astype(np.float32).astype(np.float64)
+        lo = (U - hi).astype(np.float32)  # rounded to nearest; the kernel cuts toward zero to bfloat16
+        return hi + lo.astype(np.float64)  # within 2^-31 relative of U either way
+
+    for storage in (0, 1, 2):
+        out = np.empty(4)
+        assert kh.kh_totals(np.ascontiguousarray(U).ctypes.data, nx, ny, pitch, storage, blocks, gamma, area,
+                            out.ctypes.data) == 0
+        V = held(storage)[2:-2, 2:-2]
+        r, p, u, v = V[..., 0], V[..., 1], V[..., 2], V[..., 3]
+        exact = np.array([math.fsum(x.ravel()) for x in
+                          (r, r * u, r * v, p / (gamma - 1) + 0.5 * r * (u * u + v * v))]) * area
+        scale = np.array([math.fsum(np.abs(x).ravel()) for x in (r, r * u, r * v, r)]) * area
+        tol = 1e-14 if storage < 2 else 1e-9
+        assert np.all(np.abs(out - exact) <= tol * scale), (storage, out, exact)
+        again = np.empty(4)
+        kh.kh_totals(np.ascontiguousarray(U).ctypes.data, nx, ny, pitch, storage, blocks, gamma, area,
+                     again.ctypes.data)
+        assert np.array_equal(out, again)
