@@ -320,6 +320,20 @@ class SlabSolver:
             self.fresh = True
         return self.local.get_rows(self.lo - self.l_lo, self.hi - self.lo, out=out)
 
+    def conserved_totals(self) -> np.ndarray:
+        """Mass, x momentum, y momentum and energy of the whole problem's
+        interior, in FP64 (fvm2d_get_conserved_totals): each rank's solver
+        sums its interior rows, which are exactly the rank's own rows inside
+        the problem's ghost rows (its first and last two rows are halo or
+        ghost rows), and the ranks' totals are added by an all-reduce.  The
+        sum over ranks rounds differently from one device's.  Collective."""
+        import torch
+
+        v = torch.tensor(np.asarray(self.local.conserved_totals(), dtype=np.float64),
+                         device="cuda" if self.device else "cpu")
+        self.dist.all_reduce(v, op=self.dist.ReduceOp.SUM, group=self.group)
+        return v.cpu().numpy()
+
     def gather(self) -> np.ndarray | None:
         """The whole state on rank 0 (None elsewhere).  Collective."""
         import torch

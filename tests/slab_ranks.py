@@ -73,6 +73,16 @@ class OracleSlab:
         V[a:b] = G[self.row0 + a:self.row0 + b]
         return V
 
+    def conserved_totals(self):
+        """The library's interior totals (rows and columns 2 .. n-3 of the
+        slab's array, the problem's row spacing), summed exactly."""
+        import math
+        V = self.U[2:-2, 2:-2]
+        r, p, u, v = V[..., 0], V[..., 1], V[..., 2], V[..., 3]
+        area = (self.width / self.nx) * (self.height / self.ny_global)
+        parts = (r, r * u, r * v, p / (self.gamma - 1) + 0.5 * r * (u * u + v * v))
+        return np.array([math.fsum(x.ravel()) for x in parts]) * area
+
     def get_rows(self, j0, nrows, out=None):
         R = np.ascontiguousarray(np.moveaxis(self.U[j0:j0 + nrows], -1, 0))
         if out is None:
@@ -124,9 +134,10 @@ def cpu_worker(rank, world, port, case, out_path):
         else:
             S = pkg.slab.SlabSolver(U, **kw)
         S.advance(case["steps"])
+        T = S.conserved_totals()
         G = S.gather()
         if rank == 0:  # through a file: a pipe would block on results above its 64 KB buffer
-            np.savez(out_path, G=G, t=S.t, steps=S.steps)
+            np.savez(out_path, G=G, t=S.t, steps=S.steps, totals=T)
     finally:
         dist.destroy_process_group()
 

@@ -77,3 +77,12 @@ def test_slab_run_equals_single_array_run(oracle, case, tmp_path):
                                  alpha=1.9, gamma=1.4, t_end=case["t_end"], strategy=case["strategy"])
     assert (steps, t) == (rsteps, rt)
     assert np.array_equal(G, R, equal_nan=True)
+    # the ranks' conserved totals (each its own rows) add up to the whole
+    # interior's, which the one-array run gives
+    V = R[2:-2, 2:-2]
+    r, p, u, v = V[..., 0], V[..., 1], V[..., 2], V[..., 3]
+    area = (case["width"] / case["nx"]) * (case["height"] / case["ny"])
+    parts = (r, r * u, r * v, p / 0.4 + 0.5 * r * (u * u + v * v))
+    want = np.array([np.sum(x) for x in parts]) * area
+    scale = np.array([np.sum(np.abs(x)) for x in parts]) * area
+    assert np.all(np.abs(z["totals"] - want) <= 1e-13 * scale), (z["totals"], want)
