@@ -39,6 +39,8 @@ def test_bad_arguments_fail_cleanly_without_a_device(pkg):
     assert lib.fvm2d_create(ctypes.byref(h), 4, 100) == 1
     assert b"at least 6" in lib.fvm2d_last_error()
     assert lib.fvm2d_set_cfl(None, 0.5) == 1
+    out = (ctypes.c_double * 4)()
+    assert lib.fvm2d_get_conserved_totals(None, out) == 1
     assert lib.fvm2d_destroy(None) == 0
 
 
