@@ -17,6 +17,7 @@
 
 #include "fvm2d.h"
 
+#include <array>
 #include <cstdio>
 #include <fstream>
 #include <stdexcept>
@@ -134,6 +135,16 @@ public:
     }
     double getComputationTime_ms() { return ms_; }
     int getTimeStagesCount() { return stages_; }
+    // Mass, x momentum, y momentum and energy of the last result's interior
+    // cells, summed in FP64 (fvm2d_get_conserved_totals; no reference
+    // counterpart).
+    std::array<double, 4> getConservedTotals()
+    {
+        if (!h_) throw std::runtime_error("no result: call solve() first");
+        std::array<double, 4> t{};
+        ok(fvm2d_get_conserved_totals(h_, t.data()));
+        return t;
+    }
     void writeFinalResultTo_txt(const std::string &dir)
     {
         // src/wrappers.cuh:370-397: one file per field, default stream formatting
