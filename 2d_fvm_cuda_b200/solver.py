@@ -154,6 +154,14 @@ class RGRP_2D_CUDA:
     def getTimeStagesCount(self) -> int:
         return self._stages
 
+    def getConservedTotals(self) -> np.ndarray:
+        """Mass, x momentum, y momentum and energy of the last result's
+        interior cells, summed in FP64 (fvm2d_get_conserved_totals; no
+        reference counterpart)."""
+        if self._handle is None or self._U is None:
+            raise RuntimeError("no result: call solve() first")
+        return self._handle.conserved_totals()
+
     def writeFinalResultTo_txt(self, dir: str) -> None:
         """rho_/p_/u_/v_<endTime>s.txt of the last result
         (src/wrappers.cuh:318-321); see write_matrix_txt."""

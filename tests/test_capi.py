@@ -56,3 +56,9 @@ def test_create_reports_missing_gpu(pkg):
     h = ctypes.c_void_p()
     assert lib.fvm2d_create(ctypes.byref(h), 64, 64) == 2
     assert lib.fvm2d_last_error()
+
+
+def test_python_mirror_totals_need_a_result(pkg):
+    s = pkg.RGRP_2D_CUDA()
+    with pytest.raises(RuntimeError):
+        s.getConservedTotals()
